@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Throughput of the label-indexed anisotropic elastic FDTD step on B200.
+
+Metric: Gcell-updates/s = cells x steps / device time (every cell of the grid
+counts, fluid and sponge included, as the reference counts them). One bench
+"step" is one time step of the solver over the whole workload grid.
+
+Default workload: disk_prod (160 x 256 x 256 cells, 500 grains, girdle
+fabric; see pefdtd/workloads.py), the configuration the single-solve
+throughput is quoted on. Its nine FP32 state fields are 377 MB, three times
+the 126 MB L2, so every step streams from HBM and no L2 flush is needed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank advances its own
+independent solve of the workload: a single solve does not shard, batches of
+solves do (scaling "weak"); the value is all ranks' cell updates over the
+slowest rank's device time.
+
+--impl reference runs the reference's own update kernels, compiled for the
+host CPU from the reference sources (oracle/_ref; oracle port if absent), on
+all host cores, rank 0 only, time-boxed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pulse-echo-azimuthal-simulation_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+ALG_BYTES_STEP = 74      # 9 f32 fields read + written, u16 label read, per cell-update
+ALG_BYTES_STRESS = 62    # v read 12, s read 24 + write 24, label 2
+ALG_BYTES_VEL = 50       # s read 24, v read 12 + write 12, label 2
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def _problem(workload, nt):
+    from pefdtd import workloads
+    return workloads.make_problem(workload, nt=nt)
+
+
+def _device_solve(p, nt_total):
+    from pefdtd.fdtd import DeviceSolve, _flat_probe
+    from pefdtd.damping import sponge_axis_profiles
+    shape = p["lab"].shape
+    s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float32)
+    solve = DeviceSolve(p["mats"], p["Ct"], p["rho_t"], p["h"], p["dt"], p["coeffs"], s_idx, s_w,
+                        r_off, r_idx, r_w, record=p["record"], damped_record=True,
+                        sponge=sponge_axis_profiles(shape, p["sponge"]))
+    solve.set_wavelet(p["wavelet"][:nt_total])
+    return solve
+
+
+def _e2e(p, steps):
+    """Same metric through the public C ABI host entry (pe_forward_host):
+    pinned host labels/tables/probe in, traces out, all inside the timing."""
+    import torch
+    from pefdtd import _capi
+    from pefdtd.damping import sponge_axis_profiles
+    from pefdtd.fdtd import _flat_probe
+    L = _capi.lib()
+    shape = p["lab"].shape
+    nz, ny, nx = shape
+    s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float32)
+    lab_pin = torch.from_numpy(p["mats"].astype(np.uint16).view(np.int16)).pin_memory()
+    tr_pin = torch.zeros((steps, len(r_off) - 1), dtype=torch.float32).pin_memory()
+    Ct = np.ascontiguousarray(p["Ct"], np.float32)
+    rho = np.ascontiguousarray(p["rho_t"], np.float32)
+    sp = [np.ascontiguousarray(a, np.float32) for a in sponge_axis_profiles(shape, p["sponge"])]
+    wav = np.ascontiguousarray(p["wavelet"][:steps], np.float32)
+    cfg = _capi.PeConfig()
+    cfg.nz, cfg.ny, cfg.nx = shape
+    cfg.dtype = _capi.PE_F32
+    cfg.n_coeffs = len(p["coeffs"])
+    for j, c in enumerate(p["coeffs"]):
+        cfg.coeffs[j] = float(c)
+    cfg.h, cfg.dt = p["h"], p["dt"]
+    cfg.record = _capi.REC_KIND[p["record"]]
+    cfg.damped_record = 1
+    cfg.n_mat = len(rho)
+    md = _capi.PeMedium()
+    md.ctab, md.rho = _capi.ptr(Ct), _capi.ptr(rho)
+    md.sponge_z, md.sponge_y, md.sponge_x = [_capi.ptr(a) for a in sp]
+    pr = _capi.PeProbe()
+    pr.n_src, pr.src_idx, pr.src_w = len(s_idx), _capi.ptr(s_idx), _capi.ptr(s_w)
+    pr.n_groups, pr.rec_off, pr.rec_idx, pr.rec_w = len(r_off) - 1, _capi.ptr(r_off), _capi.ptr(r_idx), _capi.ptr(r_w)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = L.pe_forward_host(_capi.C.byref(cfg), lab_pin.data_ptr(), None, _capi.C.byref(md),
+                           _capi.C.byref(pr), _capi.ptr(wav), steps, tr_pin.data_ptr())
+    el = time.perf_counter() - t0
+    _capi.check(rc)
+    ncell = nz * ny * nx
+    h2d = ncell * 2 + Ct.nbytes + rho.nbytes + sum(a.nbytes for a in sp) + wav.nbytes \
+        + s_idx.nbytes + s_w.nbytes + r_off.nbytes + r_idx.nbytes + r_w.nbytes
+    return {"value": ncell * steps / el / 1e9, "unit": "Gcell-updates/s",
+            "h2d_bytes_per_step": int(h2d // steps), "d2h_bytes_per_step": int(tr_pin.nbytes // steps),
+            "steps": steps, "wall_s": el, "api": "pe_forward_host (C ABI, host buffers)"}
+
+
+def _cpu_run(p, budget_s, max_steps):
+    """Reference kernels on the host (oracle/_ref), else the C oracle port;
+    time-boxed. Returns (Gcell/s, steps, cores, kind, sample)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    ncell = int(np.prod(p["lab"].shape))
+    kind = "reference" if O.ref_lib() is not None else "port"
+    dense = p["mats"].max() > 255
+
+    def run(nsteps):
+        q = dict(p)
+        q["nt"] = nsteps
+        q["wavelet"] = p["wavelet"][:nsteps]
+        pr = O.problem_from_workload(q, record=p["record"], damped_record=True)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            (O.run_reference_dense if dense else O.run_reference_labels)(pr, n_threads=cores)
+        else:
+            O.run_oracle(pr, n_threads=cores)
+        return time.perf_counter() - t0
+
+    t1 = run(1)                         # warm-up + sizing
+    n = int(max(2, min(max_steps, len(p["wavelet"]), budget_s / max(t1, 1e-3))))
+    el = run(n)
+    which = ("the reference's dense update kernels (strains, stress_acc, vel_update)"
+             if dense else "the reference's label-path kernels (strains_zp, stress_lab_u, vel_zp)")
+    sample = (f"{n} time steps of the full {p['name']} grid ({ncell} cells), FP32, {which} "
+              f"compiled for the host with gcc -O2 -fopenmp, {cores} threads"
+              if kind == "reference" else
+              f"{n} time steps of the full {p['name']} grid, C oracle port, {cores} threads")
+    return ncell * n / el / 1e9, n, cores, kind, sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="pefdtd", choices=["pefdtd", "reference"])
+    ap.add_argument("--workload", default="disk_prod")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    K, W = int(args.steps), max(3, int(args.warmup))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        p = _problem(args.workload, nt=max(K, 8))
+        val, n, cores, kind, sample = _cpu_run(p, budget_s=90.0, max_steps=K)
+        line = {"metric": "Gcell-updates/s", "value": val, "unit": "Gcell-updates/s",
+                "n_gpus": args.gpus, "steps": n, "warmup": 1, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": args.workload, "grid": list(p["lab"].shape),
+                           "grains": int(p["n_grains"]), "timesteps_per_step": 1},
+                "cpu_baseline": {"value": val, "unit": "Gcell-updates/s", "cores": cores,
+                                 "kind": kind, "sample": sample},
+                "e2e": {"value": val, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    p = _problem(args.workload, nt=W + K + 64)
+    ncell = int(np.prod(p["lab"].shape))
+    solve = _device_solve(p, W + K + 64)
+
+    solve.run(0, W)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        solve.run(W, W + K)
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = solve.launch_count()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    tr = solve.traces_numpy(W + K)
+    finite = bool(np.isfinite(tr).all())
+
+    # per-kernel split for the roofline (events around each launch)
+    solve.reset()
+    ms_s, ms_v = solve.profile(min(50, K))
+    solve.close()
+    peak, peak_kind = _peaks()
+    step_ms = ms / K
+    value = world * ncell * K / (ms / 1e3) / 1e9
+    dominant = "k_stress" if ms_s >= ms_v else "k_velocity"
+    dom_ms, dom_b = (ms_s, ALG_BYTES_STRESS) if dominant == "k_stress" else (ms_v, ALG_BYTES_VEL)
+    achieved = dom_b * ncell / (dom_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        traffic = tj.get(args.workload, {}).get(dominant)
+    except Exception:
+        pass
+    line = {"metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "grid": list(p["lab"].shape),
+                       "grains": int(p["n_grains"]), "h_m": p["h"], "record": p["record"],
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "state 9x4 B/cell = %.0f MB > 126 MB L2, no flush" % (36 * ncell / 1e6)},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_cell": dom_b, "peak_source": peak_kind},
+            "roofline_step": {"achieved": ALG_BYTES_STEP * ncell / (step_ms / 1e3) / 1e9,
+                              "peak": peak, "unit": "GB/s",
+                              "frac": ALG_BYTES_STEP * ncell / (step_ms / 1e3) / 1e9 / peak,
+                              "alg_bytes_per_cell": ALG_BYTES_STEP,
+                              "kernel_ms": {"k_stress": ms_s, "k_velocity": ms_v}},
+            "gpu_launches": launches, "traces_finite": finite}
+    if rank == 0 and not args.no_e2e:
+        line["e2e"] = _e2e(p, K)
+    clk_sum = clk.summary()
+    if clk_sum is not None:
+        line["clocks"] = clk_sum
+    if rank == 0 and not args.no_cpu and world == 1:
+        val, n, cores, kind, sample = _cpu_run(p, budget_s=20.0, max_steps=200)
+        line["cpu_baseline"] = {"value": val, "unit": "Gcell-updates/s", "cores": cores,
+                                "kind": kind, "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+/*
+ * pefdtd — C ABI of the B200 label-indexed anisotropic elastic FDTD solver.
+ *
+ * This is the boundary a non-Python caller binds (ctypes / cffi / cgo / JNI).
+ * It replaces the reference's solver entry point
+ *   fdtd.forward_fused_labels(lab, axes, h, dt, nt, src_pts, wavelet,
+ *                             rec_groups, order, coeffs, sponge_width,
+ *                             sponge_strength, damp_mask, c_couplant,
+ *                             rho_couplant, record, slab, stress_smem,
+ *                             progress, mat_tables)
+ *   (Jerome-Graves/pulse-echo-azimuthal-simulation sim/core/fdtd.py:1618-1816)
+ * and its dense siblings fdtd.forward_fused (:831-921) and fdtd.forward
+ * (:236-376), which the reference drives through CuPy RawKernel launches
+ * (:586-591, :1786-1815). Everything crossing this boundary is a plain
+ * pointer, size or enum; no PyTorch or CuPy type appears.
+ *
+ * Conventions
+ *  - Grids are (nz, ny, nx), C order, x fastest; flat cell index
+ *    i = (iz * ny + iy) * nx + ix (the reference's np.ravel_multi_index).
+ *  - "dev" pointers are CUDA device memory on the current device; all other
+ *    pointers are host memory, read during the call only.
+ *  - Material index m is the reference's (label + 1): m = 0 is the fluid
+ *    couplant, m = g + 1 is grain g. At most PE_MAX_MATERIALS materials.
+ *  - Every function returns PE_OK or an error code; pe_last_error() gives the
+ *    message of the last failure on the calling thread. PE_ERR_INVALID is the
+ *    condition the reference reports as ValueError.
+ */
+#ifndef PEFDTD_H
+#define PEFDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PE_ABI_VERSION 1
+#define PE_MAX_MATERIALS 16383
+
+enum PeStatus {
+    PE_OK = 0,
+    PE_ERR_INVALID = 1,     /* bad argument (reference: ValueError) */
+    PE_ERR_CUDA = 2,        /* CUDA runtime error */
+    PE_ERR_NOMEM = 3,       /* device or host allocation failed */
+    PE_ERR_UNSUPPORTED = 4, /* valid request this build cannot serve */
+    PE_ERR_TIMEOUT = 5      /* a bounded device-side wait gave up */
+};
+
+enum PeDtype { PE_F32 = 0, PE_F64 = 1 };
+
+/* What a receiver records (reference `record=`, sim/core/fdtd.py:1806-1812). */
+enum PeRecord { PE_REC_PRESSURE = 0, PE_REC_VX = 1, PE_REC_VY = 2, PE_REC_VZ = 3 };
+
+/* Solve description. Scalars only. */
+typedef struct PeConfig {
+    int32_t nz, ny, nx;
+    int32_t dtype;          /* PeDtype: arithmetic of fields, tables, traces */
+    int32_t n_coeffs;       /* 1..4 staggered coefficients (order = 2 * n) */
+    double coeffs[4];       /* reference `coeffs` (optimised_coeffs(order)) */
+    double h, dt;           /* grid step [m], time step [s] */
+    int32_t record;         /* PeRecord */
+    int32_t damped_record;  /* 0: pressure from the stored (pre-deferred-
+                               damping) stress, as forward_fused_labels;
+                               1: from the end-of-step damped stress, as
+                               forward_fused / forward (:909-915, :361-367) */
+    int32_t n_mat;          /* rows in the material tables, 1..PE_MAX_MATERIALS */
+    int32_t chunk_steps;    /* steps per captured CUDA graph (0 = 200) */
+    int32_t tile_x, tile_y; /* kernel tile (0 = tuned default) */
+    int32_t z_chunk;        /* planes per z-march (0 = tuned default) */
+} PeConfig;
+
+/* The medium. Volumes live on the device; tables are small host arrays. */
+typedef struct PeMedium {
+    const uint16_t *labels_dev;    /* (nz, ny, nx) material index (< n_mat) */
+    const float *damp_volume_dev;  /* (nz, ny, nx) f32 per-step multiplier
+                                      (reference damp_mask) or NULL */
+    const void *ctab;              /* (n_mat, 36) dtype: full symmetric Voigt
+                                      rows, row-major I*6+J (reference Ct) */
+    const void *rho;               /* (n_mat,) dtype density (reference rho_t) */
+    const float *sponge_z;         /* (nz,) f32 sponge taper or NULL */
+    const float *sponge_y;         /* (ny,) */
+    const float *sponge_x;         /* (nx,); all three or none. The damping
+                                      applied to a cell is
+                                      ((sz*sy)*sx)*volume in f32, the
+                                      reference's sponge_profile(..)*damp_mask */
+} PeMedium;
+
+/* Source and receivers (host arrays, copied at create). */
+typedef struct PeProbe {
+    int32_t n_src;
+    const int64_t *src_idx;  /* flat cell index; s1,s2,s3 += wavelet[n]*w after
+                                the stress update (reference :1798-1800). A
+                                repeated cell keeps its last entry. */
+    const void *src_w;       /* (n_src,) dtype */
+    int32_t n_groups;        /* receiver groups = trace columns */
+    const int64_t *rec_off;  /* (n_groups + 1) CSR offsets into rec_idx/rec_w */
+    const int64_t *rec_idx;  /* flat cell index per entry */
+    const void *rec_w;       /* dtype weight per entry; a trace sample is the
+                                weighted sum over its group, in list order */
+} PeProbe;
+
+/* The nine state fields, device memory of dtype, (nz, ny, nx) each. */
+typedef struct PeState {
+    void *v[3];  /* vx, vy, vz */
+    void *s[6];  /* s1..s6 (Voigt order xx, yy, zz, yz, xz, xy) */
+} PeState;
+
+typedef struct PeSolver PeSolver;
+
+/* ABI version of the loaded library (PE_ABI_VERSION). */
+int pe_abi_version(void);
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char *pe_last_error(void);
+
+/* Validate and prepare a solve: copies the labels (marking source and
+ * receiver cells), tables, profiles and probe into solver-owned device
+ * memory. labels out of range -> PE_ERR_INVALID (reference :1650-1658,
+ * :1674-1677); n_coeffs outside 1..4 -> PE_ERR_INVALID (:1638-1643). */
+int pe_solver_create(const PeConfig *cfg, const PeMedium *medium, const PeProbe *probe,
+                     PeSolver **out);
+
+/* Upload the source wavelet (host, dtype, nt samples). */
+int pe_solver_set_wavelet(PeSolver *s, const void *wavelet, int64_t nt);
+
+/* Advance `state` over steps [step_begin, step_end) on `stream`
+ * (cudaStream_t, NULL = legacy default stream) and write trace rows
+ * traces_dev[n * n_groups + g] for those steps (traces_dev: device, dtype,
+ * at least step_end * n_groups elements). Asynchronous with respect to the
+ * host. Full chunks run as one captured CUDA graph each. */
+int pe_solver_run(PeSolver *s, const PeState *state, void *traces_dev, int64_t step_begin,
+                  int64_t step_end, void *stream);
+
+/* Kernel launches issued by the last pe_solver_run (diagnostics). */
+int64_t pe_solver_launch_count(const PeSolver *s);
+
+/* Diagnostics for roofline reporting: advance `state` by n_steps from step 0
+ * one kernel at a time, with CUDA events around each launch, and write the
+ * mean per-step milliseconds of the stress and velocity kernels to
+ * ms_out[0], ms_out[1]. Synchronous. No reference counterpart (the
+ * reference times whole solves with time.time()). */
+int pe_solver_profile(PeSolver *s, const PeState *state, int n_steps, float *ms_out,
+                      void *stream);
+
+int pe_solver_destroy(PeSolver *s);
+
+/* One call, host buffers in and out: the reference's forward_fused_labels
+ * contract for callers without device memory management. Allocates the
+ * state on the device, zeroes it, runs nt steps and copies the (nt, n_groups)
+ * traces (dtype) back into traces_host. labels_host is (nz, ny, nx) uint16,
+ * damp_volume_host f32 or NULL; medium->labels_dev/damp_volume_dev are
+ * ignored. */
+int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host,
+                    const float *damp_volume_host, const PeMedium *medium,
+                    const PeProbe *probe, const void *wavelet_host, int64_t nt,
+                    void *traces_host);
+
+/* Power-diagram labels of a cylinder (specimen builder, reference
+ * sim/core/specimen.py:298-337): out_dev[(iz*ny + iy)*nx + ix] = the seed
+ * minimising ((x-sx)^2 + (y-sy)^2) - w + (z-sz)^2 in float64 at point
+ * (xs[ix], ys[iy], zs[iz]), first index on ties, or -1 where
+ * x^2 + y^2 > R2. seeds (ns, 3) and weights (ns, NULL = 0) are host arrays;
+ * out_dev is device int32. Synchronous on `stream`. */
+int pe_label_cylinder(const double *xs, int nx, const double *ys, int ny, const double *zs,
+                      int nz, double R2, const double *seeds, const double *weights, int ns,
+                      int32_t *out_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PEFDTD_H */

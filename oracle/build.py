@@ -1,0 +1,100 @@
+"""TEST INFRASTRUCTURE ONLY — build recipe for the CPU oracle and the
+reference-kernel harness.
+
+* ``oracle/_build/liboracle.so``  from oracle/fdtd_oracle.c (the C restatement).
+* ``oracle/_ref/libref_cpu.so``   from oracle/ref_harness.cpp plus the
+  reference's own CUDA-C kernel strings, read from the reference module where
+  it lies (``sim/core/fdtd.py`` of Jerome-Graves/pulse-echo-azimuthal-simulation)
+  and written to ``oracle/_ref/ref_kernels.inc``. Only possible where the
+  reference tree is present; elsewhere the prebuilt library is used.
+
+Both outputs are git-ignored. Flags: no fast-math and no FP contraction, so
+every product and sum is rounded as written; no ``-march=native`` so the
+library runs on any x86-64 host it is copied to.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_OUT = os.path.join(HERE, "_ref")
+REFERENCE_ROOT = os.environ.get("PE_REFERENCE_ROOT", "/root/reference")
+
+ORACLE_LIB = os.path.join(BUILD, "liboracle.so")
+REF_CPU_LIB = os.path.join(REF_OUT, "libref_cpu.so")
+
+_CFLAGS = ["-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared", "-Wall",
+           "-Wno-unused-function"]
+
+
+def _newer(target, sources):
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(s) <= t for s in sources if os.path.exists(s))
+
+
+def build_oracle(force=False):
+    srcs = [os.path.join(HERE, "fdtd_oracle.c"), os.path.join(HERE, "fdtd_oracle_impl.h")]
+    if not force and _newer(ORACLE_LIB, srcs):
+        return ORACLE_LIB
+    os.makedirs(BUILD, exist_ok=True)
+    tmp = ORACLE_LIB + ".tmp"
+    subprocess.check_call(["gcc", *_CFLAGS, "-o", tmp, srcs[0], "-lm"])
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def _reference_kernel_sources(root):
+    """The reference's own kernel source strings, unmodified, from the module."""
+    sys.path.insert(0, os.path.join(root, "sim", "core"))
+    sys.path.insert(0, os.path.join(root, "vendor"))
+    try:
+        import importlib
+        fd = importlib.import_module("fdtd")
+        parts = [
+            ("strains_zp (sim/core/fdtd.py:1102-1177)", fd._STRAIN_ZP_SRC),
+            ("stress_lab_u (sim/core/fdtd.py:594-689)", fd._stress_unrolled_src()),
+            ("vel_zp (sim/core/fdtd.py:1179-1257)", fd._VEL_ZP_SRC),
+            ("strains (sim/core/fdtd.py:463-505)", fd._STRAIN_SRC),
+            ("stress_acc (sim/core/fdtd.py:507-583)", fd._STRESS_SRC),
+            ("vel_update (sim/core/fdtd.py:392-442)", fd._VEL_SRC),
+        ]
+    finally:
+        sys.path.pop(0)
+        sys.path.pop(0)
+    out = ["// GENERATED by oracle/build.py from the reference module; do not commit.\n"]
+    for name, src in parts:
+        out.append(f"\n// ---- {name}\n")
+        out.append(src)
+    return "".join(out)
+
+
+def build_ref(force=False):
+    """Build oracle/_ref/libref_cpu.so; returns its path or None if impossible."""
+    core = os.path.join(REFERENCE_ROOT, "sim", "core", "fdtd.py")
+    harness = os.path.join(HERE, "ref_harness.cpp")
+    if not os.path.exists(core):
+        return REF_CPU_LIB if os.path.exists(REF_CPU_LIB) else None
+    if not force and _newer(REF_CPU_LIB, [core, harness, __file__]):
+        return REF_CPU_LIB
+    os.makedirs(REF_OUT, exist_ok=True)
+    inc = os.path.join(REF_OUT, "ref_kernels.inc")
+    with open(inc, "w") as f:
+        f.write(_reference_kernel_sources(REFERENCE_ROOT))
+    tmp = REF_CPU_LIB + ".tmp"
+    subprocess.check_call(["g++", "-std=c++17", *_CFLAGS, "-Wno-unused-variable",
+                           "-I", HERE, "-o", tmp, harness])
+    os.replace(tmp, REF_CPU_LIB)
+    return REF_CPU_LIB
+
+
+def build_all(force=False):
+    return build_oracle(force), build_ref(force)
+
+
+if __name__ == "__main__":
+    print(build_all(force="--force" in sys.argv))

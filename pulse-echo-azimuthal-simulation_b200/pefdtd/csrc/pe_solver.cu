@@ -1,0 +1,572 @@
+// C ABI and runtime of the B200 FDTD solver (include/pefdtd.h).
+//
+// The runtime owns everything a solve needs besides the nine state fields:
+// the flagged label volume, tables, damping, probe lists, the receiver
+// sample buffer of one chunk and a device step counter. A chunk of
+// `chunk_steps` steps (stress + velocity launch per step, then one trace
+// reduction and a counter advance) is captured once as a CUDA graph and
+// replayed; the kernels read the global step from the device counter, so the
+// same graph serves every chunk. This is the reference's Python step loop
+// (sim/core/fdtd.py:1786-1816) moved onto the device.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pe_kernels.cuh"
+#include "pefdtd.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define PE_CUDA(expr)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? PE_ERR_NOMEM : PE_ERR_CUDA,      \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+template <typename P>
+int dev_alloc(P **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess)
+        return fail(PE_ERR_NOMEM, std::string("cudaMalloc(") + std::to_string(bytes) +
+                                      "): " + cudaGetErrorString(e));
+    return PE_OK;
+}
+
+int dtype_size(int dtype) { return dtype == PE_F64 ? 8 : 4; }
+
+struct TileShape {
+    int tx, ty;
+};
+
+}  // namespace
+
+struct PeSolver {
+    PeConfig cfg{};
+    long long ncell = 0;
+    int esize = 4;
+    // device buffers owned by the solver
+    uint16_t *lab = nullptr;
+    void *c21 = nullptr, *rho = nullptr;
+    float *dz = nullptr, *dy = nullptr, *dx = nullptr, *dvol = nullptr;
+    long long *src_idx = nullptr;
+    void *src_w = nullptr;
+    int n_src = 0;
+    long long *rec_cell = nullptr;
+    int *rec_pos = nullptr;
+    void *rec_w = nullptr;
+    long long *grp_off = nullptr;
+    int n_rec = 0, n_groups = 0;
+    void *rec_val = nullptr;
+    void *wavelet = nullptr;
+    long long nt_wav = 0;
+    long long *step = nullptr;
+    // execution
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    PeState gstate{};
+    void *gtraces = nullptr;
+    int chunk = 200;
+    int tx = 32, ty = 8, zc = 0;
+    long long launches = 0;
+
+    ~PeSolver()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
+        if (stream) cudaStreamDestroy(stream);
+        void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
+                        rec_pos, rec_w, grp_off, rec_val, wavelet, step};
+        for (void *b : bufs)
+            if (b) cudaFree(b);
+    }
+};
+
+namespace {
+
+template <typename T>
+pe::StepArgs<T> make_args(const PeSolver *S, const PeState *st, int k)
+{
+    pe::StepArgs<T> A{};
+    for (int i = 0; i < 3; ++i) A.v[i] = (T *)st->v[i];
+    for (int i = 0; i < 6; ++i) A.s[i] = (T *)st->s[i];
+    A.lab = S->lab;
+    A.c21 = (const T *)S->c21;
+    A.rho = (const T *)S->rho;
+    A.dz = S->dz;
+    A.dy = S->dy;
+    A.dx = S->dx;
+    A.dvol = S->dvol;
+    A.nz = S->cfg.nz;
+    A.ny = S->cfg.ny;
+    A.nx = S->cfg.nx;
+    A.sy = S->cfg.nx;
+    A.sz = (long long)S->cfg.nx * S->cfg.ny;
+    for (int j = 0; j < 4; ++j) A.c[j] = j < S->cfg.n_coeffs ? (T)S->cfg.coeffs[j] : T(0);
+    A.nc = S->cfg.n_coeffs;
+    A.inv_h = (T)(1.0 / S->cfg.h);
+    A.dt = (T)S->cfg.dt;
+    A.dt_h = (T)(S->cfg.dt / S->cfg.h);
+    A.src_idx = S->src_idx;
+    A.src_w = (const T *)S->src_w;
+    A.n_src = S->n_src;
+    A.wavelet = (const T *)S->wavelet;
+    A.rec_cell = S->rec_cell;
+    A.rec_pos = S->rec_pos;
+    A.n_rec = S->n_rec;
+    A.rec_val = (T *)S->rec_val;
+    A.rec_kind = S->cfg.record;
+    A.rec_damped = S->cfg.damped_record;
+    A.step = S->step;
+    A.k = k;
+    A.zc = S->zc;
+    return A;
+}
+
+template <typename T, int TX, int TY>
+void launch_pair(const pe::StepArgs<T> &A, cudaStream_t st)
+{
+    dim3 block(TX, TY, 1);
+    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + A.zc - 1) / A.zc);
+    pe::k_stress<T, TX, TY><<<grid, block, 0, st>>>(A);
+    pe::k_velocity<T, TX, TY><<<grid, block, 0, st>>>(A);
+}
+
+template <typename T>
+int launch_chunk_t(PeSolver *S, const PeState *st, void *traces, int len)
+{
+    for (int k = 0; k < len; ++k) {
+        pe::StepArgs<T> A = make_args<T>(S, st, k);
+        if (S->tx == 32 && S->ty == 8) launch_pair<T, 32, 8>(A, S->stream);
+        else launch_pair<T, 32, 4>(A, S->stream);
+        S->launches += 2;
+    }
+    if (S->n_groups > 0) {
+        const int nthr = len * S->n_groups;
+        pe::k_reduce_traces<T><<<(nthr + 127) / 128, 128, 0, S->stream>>>(
+            (const T *)S->rec_val, (const T *)S->rec_w, S->grp_off, S->n_groups, S->n_rec, len,
+            S->step, (T *)traces);
+        S->launches += 1;
+    }
+    pe::k_step_advance<<<1, 1, 0, S->stream>>>(S->step, len);
+    S->launches += 1;
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+int launch_chunk(PeSolver *S, const PeState *st, void *traces, int len)
+{
+    return S->cfg.dtype == PE_F64 ? launch_chunk_t<double>(S, st, traces, len)
+                                  : launch_chunk_t<float>(S, st, traces, len);
+}
+
+bool same_state(const PeState &a, const PeState &b)
+{
+    for (int i = 0; i < 3; ++i)
+        if (a.v[i] != b.v[i]) return false;
+    for (int i = 0; i < 6; ++i)
+        if (a.s[i] != b.s[i]) return false;
+    return true;
+}
+
+int pick_zchunk(const PeSolver *S)
+{
+    if (S->cfg.z_chunk > 0) return S->cfg.z_chunk;
+    // enough blocks to give every SM several, without short marches
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (long long)((S->cfg.nx + S->tx - 1) / S->tx) *
+                            ((S->cfg.ny + S->ty - 1) / S->ty);
+    const long long want = 4LL * nsm;
+    long long nchunks = (want + tiles - 1) / tiles;
+    int zc = (int)((S->cfg.nz + nchunks - 1) / nchunks);
+    if (zc < 16) zc = 16;
+    if (zc > S->cfg.nz) zc = S->cfg.nz;
+    return zc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pe_abi_version(void) { return PE_ABI_VERSION; }
+
+const char *pe_last_error(void) { return g_err.c_str(); }
+
+int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr, PeSolver **out)
+{
+    if (!cfg || !md || !pr || !out) return fail(PE_ERR_INVALID, "null argument");
+    *out = nullptr;
+    const PeConfig &c = *cfg;
+    if (c.nz < 1 || c.ny < 1 || c.nx < 1)
+        return fail(PE_ERR_INVALID, "grid dimensions must be positive");
+    if (c.n_coeffs < 1 || c.n_coeffs > 4)
+        return fail(PE_ERR_INVALID,
+                    "supports order <= 8 (" + std::to_string(c.n_coeffs) +
+                        " coefficients given): the kernels carry +/-4 taps per axis");
+    if (c.dtype != PE_F32 && c.dtype != PE_F64) return fail(PE_ERR_INVALID, "dtype must be F32 or F64");
+    if (c.record < 0 || c.record > 3) return fail(PE_ERR_INVALID, "record must be 0..3");
+    if (c.n_mat < 1 || c.n_mat > PE_MAX_MATERIALS)
+        return fail(PE_ERR_INVALID, "n_mat must lie in [1, " + std::to_string(PE_MAX_MATERIALS) + "]");
+    if (!(c.h > 0) || !(c.dt > 0)) return fail(PE_ERR_INVALID, "h and dt must be positive");
+    if (!md->labels_dev || !md->ctab || !md->rho)
+        return fail(PE_ERR_INVALID, "labels_dev, ctab and rho are required");
+    const bool any_sp = md->sponge_z || md->sponge_y || md->sponge_x;
+    const bool all_sp = md->sponge_z && md->sponge_y && md->sponge_x;
+    if (any_sp && !all_sp) return fail(PE_ERR_INVALID, "give all three sponge profiles or none");
+    if (pr->n_src < 0 || pr->n_groups < 0) return fail(PE_ERR_INVALID, "negative probe sizes");
+    if (pr->n_src > 0 && (!pr->src_idx || !pr->src_w)) return fail(PE_ERR_INVALID, "source arrays missing");
+    if (pr->n_groups > 0 && (!pr->rec_off || !pr->rec_idx || !pr->rec_w))
+        return fail(PE_ERR_INVALID, "receiver arrays missing");
+
+    std::unique_ptr<PeSolver> S(new PeSolver());
+    S->cfg = c;
+    S->ncell = (long long)c.nz * c.ny * c.nx;
+    S->esize = dtype_size(c.dtype);
+    S->chunk = c.chunk_steps > 0 ? c.chunk_steps : 200;
+    if (c.tile_x > 0 && c.tile_y > 0) {
+        const TileShape ok[] = {{32, 8}, {32, 4}};
+        bool found = false;
+        for (auto t : ok) found |= (t.tx == c.tile_x && t.ty == c.tile_y);
+        if (!found) return fail(PE_ERR_UNSUPPORTED, "tile shape not compiled in");
+        S->tx = c.tile_x;
+        S->ty = c.tile_y;
+    }
+    S->zc = pick_zchunk(S.get());
+    const long long ncell = S->ncell;
+    const int es = S->esize;
+
+    // ---- probe lists (host side: validate, dedupe, sort)
+    std::vector<long long> sidx;
+    std::vector<char> swb;
+    {
+        std::map<long long, int> last;  // cell -> last entry
+        for (int k = 0; k < pr->n_src; ++k) {
+            const long long q = pr->src_idx[k];
+            if (q < 0 || q >= ncell)
+                return fail(PE_ERR_INVALID, "source cell index " + std::to_string(q) + " outside the grid");
+            last[q] = k;
+        }
+        for (auto &kv : last) {
+            sidx.push_back(kv.first);
+            const char *w = (const char *)pr->src_w + (size_t)kv.second * es;
+            swb.insert(swb.end(), w, w + es);
+        }
+    }
+    S->n_src = (int)sidx.size();
+    std::vector<long long> roff, rcell_sorted;
+    std::vector<int> rpos_sorted;
+    S->n_groups = pr->n_groups;
+    long long n_rec = 0;
+    if (pr->n_groups > 0) {
+        if (pr->rec_off[0] != 0) return fail(PE_ERR_INVALID, "rec_off[0] must be 0");
+        for (int g = 0; g < pr->n_groups; ++g)
+            if (pr->rec_off[g + 1] < pr->rec_off[g]) return fail(PE_ERR_INVALID, "rec_off must be non-decreasing");
+        n_rec = pr->rec_off[pr->n_groups];
+        if (n_rec > (1LL << 30)) return fail(PE_ERR_INVALID, "too many receiver entries");
+        std::vector<std::pair<long long, int>> ent((size_t)n_rec);
+        for (long long e = 0; e < n_rec; ++e) {
+            const long long q = pr->rec_idx[e];
+            if (q < 0 || q >= ncell)
+                return fail(PE_ERR_INVALID, "receiver cell index " + std::to_string(q) + " outside the grid");
+            ent[(size_t)e] = {q, (int)e};
+        }
+        std::sort(ent.begin(), ent.end());
+        for (auto &p : ent) {
+            rcell_sorted.push_back(p.first);
+            rpos_sorted.push_back(p.second);
+        }
+        roff.assign(pr->rec_off, pr->rec_off + pr->n_groups + 1);
+    }
+    S->n_rec = (int)n_rec;
+
+    PE_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    PE_CUDA(cudaEventCreateWithFlags(&S->ev_in, cudaEventDisableTiming));
+    PE_CUDA(cudaEventCreateWithFlags(&S->ev_out, cudaEventDisableTiming));
+    cudaStream_t st = S->stream;
+
+    int rc;
+    if ((rc = dev_alloc(&S->lab, sizeof(uint16_t) * ncell))) return rc;
+    if ((rc = dev_alloc(&S->c21, (size_t)es * pe::C21_STRIDE * c.n_mat))) return rc;
+    if ((rc = dev_alloc(&S->rho, (size_t)es * c.n_mat))) return rc;
+    if ((rc = dev_alloc(&S->step, sizeof(long long)))) return rc;
+
+    // labels: copy + range check, then mark source / receiver cells
+    unsigned long long *nbad = nullptr;
+    if ((rc = dev_alloc(&nbad, sizeof(unsigned long long)))) return rc;
+    PE_CUDA(cudaMemsetAsync(nbad, 0, sizeof(unsigned long long), st));
+    pe::k_labels_copy<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(md->labels_dev, S->lab, ncell,
+                                                                       c.n_mat, nbad);
+    unsigned long long bad = 0;
+    PE_CUDA(cudaMemcpyAsync(&bad, nbad, sizeof(bad), cudaMemcpyDeviceToHost, st));
+    PE_CUDA(cudaStreamSynchronize(st));
+    cudaFree(nbad);
+    if (bad)
+        return fail(PE_ERR_INVALID, std::to_string(bad) + " cells carry a material index >= n_mat (" +
+                                        std::to_string(c.n_mat) + "): label has no table row");
+
+    // tables
+    {
+        void *c36 = nullptr;
+        if ((rc = dev_alloc(&c36, (size_t)es * 36 * c.n_mat))) return rc;
+        PE_CUDA(cudaMemcpyAsync(c36, md->ctab, (size_t)es * 36 * c.n_mat, cudaMemcpyHostToDevice, st));
+        if (c.dtype == PE_F64)
+            pe::k_c36_to_c21<double><<<(c.n_mat + 127) / 128, 128, 0, st>>>((const double *)c36, (double *)S->c21, c.n_mat);
+        else
+            pe::k_c36_to_c21<float><<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)c36, (float *)S->c21, c.n_mat);
+        PE_CUDA(cudaMemcpyAsync(S->rho, md->rho, (size_t)es * c.n_mat, cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaStreamSynchronize(st));
+        cudaFree(c36);
+    }
+    if (all_sp) {
+        if ((rc = dev_alloc(&S->dz, sizeof(float) * c.nz))) return rc;
+        if ((rc = dev_alloc(&S->dy, sizeof(float) * c.ny))) return rc;
+        if ((rc = dev_alloc(&S->dx, sizeof(float) * c.nx))) return rc;
+        PE_CUDA(cudaMemcpyAsync(S->dz, md->sponge_z, sizeof(float) * c.nz, cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaMemcpyAsync(S->dy, md->sponge_y, sizeof(float) * c.ny, cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaMemcpyAsync(S->dx, md->sponge_x, sizeof(float) * c.nx, cudaMemcpyHostToDevice, st));
+    }
+    if (md->damp_volume_dev) {
+        if ((rc = dev_alloc(&S->dvol, sizeof(float) * ncell))) return rc;
+        PE_CUDA(cudaMemcpyAsync(S->dvol, md->damp_volume_dev, sizeof(float) * ncell, cudaMemcpyDeviceToDevice, st));
+    }
+    // probe
+    if ((rc = dev_alloc(&S->src_idx, sizeof(long long) * std::max<size_t>(1, sidx.size())))) return rc;
+    if ((rc = dev_alloc(&S->src_w, (size_t)es * std::max<size_t>(1, sidx.size())))) return rc;
+    if (!sidx.empty()) {
+        PE_CUDA(cudaMemcpyAsync(S->src_idx, sidx.data(), sizeof(long long) * sidx.size(), cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaMemcpyAsync(S->src_w, swb.data(), swb.size(), cudaMemcpyHostToDevice, st));
+        pe::k_labels_flag<<<(S->n_src + 127) / 128, 128, 0, st>>>(S->lab, S->src_idx, S->n_src, pe::LAB_SRC);
+    }
+    const size_t nr = (size_t)std::max<long long>(1, n_rec);
+    if ((rc = dev_alloc(&S->rec_cell, sizeof(long long) * nr))) return rc;
+    if ((rc = dev_alloc(&S->rec_pos, sizeof(int) * nr))) return rc;
+    if ((rc = dev_alloc(&S->rec_w, (size_t)es * nr))) return rc;
+    if ((rc = dev_alloc(&S->grp_off, sizeof(long long) * (S->n_groups + 1)))) return rc;
+    if ((rc = dev_alloc(&S->rec_val, (size_t)es * nr * S->chunk))) return rc;
+    PE_CUDA(cudaMemsetAsync(S->rec_val, 0, (size_t)es * nr * S->chunk, st));
+    if (n_rec > 0) {
+        PE_CUDA(cudaMemcpyAsync(S->rec_cell, rcell_sorted.data(), sizeof(long long) * n_rec, cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaMemcpyAsync(S->rec_pos, rpos_sorted.data(), sizeof(int) * n_rec, cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaMemcpyAsync(S->rec_w, pr->rec_w, (size_t)es * n_rec, cudaMemcpyHostToDevice, st));
+        pe::k_labels_flag<<<(unsigned)((n_rec + 127) / 128), 128, 0, st>>>(S->lab, S->rec_cell, (int)n_rec, pe::LAB_REC);
+    }
+    if (S->n_groups > 0)
+        PE_CUDA(cudaMemcpyAsync(S->grp_off, roff.data(), sizeof(long long) * (S->n_groups + 1), cudaMemcpyHostToDevice, st));
+    PE_CUDA(cudaStreamSynchronize(st));
+    PE_CUDA(cudaGetLastError());
+    *out = S.release();
+    return PE_OK;
+}
+
+int pe_solver_set_wavelet(PeSolver *S, const void *wavelet, int64_t nt)
+{
+    if (!S || (nt > 0 && !wavelet) || nt < 0) return fail(PE_ERR_INVALID, "bad wavelet");
+    if (S->wavelet) {
+        cudaFree(S->wavelet);
+        S->wavelet = nullptr;
+    }
+    int rc = dev_alloc(&S->wavelet, (size_t)S->esize * std::max<int64_t>(1, nt));
+    if (rc) return rc;
+    if (nt > 0)
+        PE_CUDA(cudaMemcpyAsync(S->wavelet, wavelet, (size_t)S->esize * nt, cudaMemcpyHostToDevice, S->stream));
+    PE_CUDA(cudaStreamSynchronize(S->stream));
+    S->nt_wav = nt;
+    return PE_OK;
+}
+
+int pe_solver_run(PeSolver *S, const PeState *state, void *traces, int64_t b, int64_t e, void *stream)
+{
+    if (!S || !state) return fail(PE_ERR_INVALID, "null argument");
+    if (b < 0 || e < b) return fail(PE_ERR_INVALID, "need 0 <= step_begin <= step_end");
+    if (e > S->nt_wav && S->n_src > 0)
+        return fail(PE_ERR_INVALID, "step_end " + std::to_string(e) + " beyond the wavelet (" +
+                                        std::to_string(S->nt_wav) + " samples)");
+    if (S->n_groups > 0 && !traces) return fail(PE_ERR_INVALID, "traces buffer required");
+    for (int i = 0; i < 3; ++i)
+        if (!state->v[i]) return fail(PE_ERR_INVALID, "state field missing");
+    for (int i = 0; i < 6; ++i)
+        if (!state->s[i]) return fail(PE_ERR_INVALID, "state field missing");
+    S->launches = 0;
+    if (e == b) return PE_OK;
+    cudaStream_t user = (cudaStream_t)stream;
+    PE_CUDA(cudaEventRecord(S->ev_in, user));
+    PE_CUDA(cudaStreamWaitEvent(S->stream, S->ev_in, 0));
+    pe::k_step_set<<<1, 1, 0, S->stream>>>(S->step, b);
+    S->launches += 1;
+    int64_t n = b;
+    while (n < e) {
+        const int len = (int)std::min<int64_t>(S->chunk, e - n);
+        if (len == S->chunk) {
+            if (!S->gexec || !same_state(S->gstate, *state) || S->gtraces != traces) {
+                if (S->gexec) {
+                    cudaGraphExecDestroy(S->gexec);
+                    S->gexec = nullptr;
+                }
+                cudaGraph_t g = nullptr;
+                PE_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+                const long long before = S->launches;
+                int rc = launch_chunk(S, state, traces, len);
+                cudaError_t ce = cudaStreamEndCapture(S->stream, &g);
+                if (rc) return rc;
+                if (ce != cudaSuccess) return fail(PE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+                S->launches = before;
+                ce = cudaGraphInstantiate(&S->gexec, g, 0);
+                cudaGraphDestroy(g);
+                if (ce != cudaSuccess) return fail(PE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+                S->gstate = *state;
+                S->gtraces = traces;
+            }
+            PE_CUDA(cudaGraphLaunch(S->gexec, S->stream));
+            S->launches += 2LL * len + (S->n_groups > 0 ? 1 : 0) + 1;
+        } else {
+            int rc = launch_chunk(S, state, traces, len);
+            if (rc) return rc;
+        }
+        n += len;
+    }
+    PE_CUDA(cudaEventRecord(S->ev_out, S->stream));
+    PE_CUDA(cudaStreamWaitEvent(user, S->ev_out, 0));
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+int64_t pe_solver_launch_count(const PeSolver *S) { return S ? S->launches : -1; }
+
+int pe_solver_profile(PeSolver *S, const PeState *state, int n_steps, float *ms_out, void *stream)
+{
+    if (!S || !state || !ms_out || n_steps < 1) return fail(PE_ERR_INVALID, "bad profile request");
+    if (S->n_src > 0 && S->nt_wav < n_steps) return fail(PE_ERR_INVALID, "wavelet shorter than n_steps");
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaEvent_t ev[3];
+    for (auto &e : ev) PE_CUDA(cudaEventCreate(&e));
+    PE_CUDA(cudaEventRecord(S->ev_in, user));
+    PE_CUDA(cudaStreamWaitEvent(S->stream, S->ev_in, 0));
+    pe::k_step_set<<<1, 1, 0, S->stream>>>(S->step, 0);
+    float tot_s = 0.f, tot_v = 0.f;
+    const int saved_chunk = S->chunk;
+    for (int n = 0; n < n_steps; ++n) {
+        // one step at a time with events around each kernel (no graph)
+        PE_CUDA(cudaEventRecord(ev[0], S->stream));
+        if (S->cfg.dtype == PE_F64) {
+            pe::StepArgs<double> A = make_args<double>(S, state, 0);
+            dim3 grid((A.nx + S->tx - 1) / S->tx, (A.ny + S->ty - 1) / S->ty, (A.nz + A.zc - 1) / A.zc);
+            if (S->ty == 8) pe::k_stress<double, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
+            else pe::k_stress<double, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+            PE_CUDA(cudaEventRecord(ev[1], S->stream));
+            if (S->ty == 8) pe::k_velocity<double, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
+            else pe::k_velocity<double, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+        } else {
+            pe::StepArgs<float> A = make_args<float>(S, state, 0);
+            dim3 grid((A.nx + S->tx - 1) / S->tx, (A.ny + S->ty - 1) / S->ty, (A.nz + A.zc - 1) / A.zc);
+            if (S->ty == 8) pe::k_stress<float, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
+            else pe::k_stress<float, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+            PE_CUDA(cudaEventRecord(ev[1], S->stream));
+            if (S->ty == 8) pe::k_velocity<float, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
+            else pe::k_velocity<float, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+        }
+        PE_CUDA(cudaEventRecord(ev[2], S->stream));
+        pe::k_step_advance<<<1, 1, 0, S->stream>>>(S->step, 1);
+        PE_CUDA(cudaEventSynchronize(ev[2]));
+        float a = 0.f, b = 0.f;
+        PE_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+        PE_CUDA(cudaEventElapsedTime(&b, ev[1], ev[2]));
+        tot_s += a;
+        tot_v += b;
+    }
+    S->chunk = saved_chunk;
+    for (auto &e : ev) cudaEventDestroy(e);
+    PE_CUDA(cudaEventRecord(S->ev_out, S->stream));
+    PE_CUDA(cudaStreamWaitEvent(user, S->ev_out, 0));
+    ms_out[0] = tot_s / n_steps;
+    ms_out[1] = tot_v / n_steps;
+    return PE_OK;
+}
+
+int pe_solver_destroy(PeSolver *S)
+{
+    if (S) {
+        cudaStreamSynchronize(S->stream);
+        delete S;
+    }
+    return PE_OK;
+}
+
+int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host, const float *damp_host,
+                    const PeMedium *medium, const PeProbe *probe, const void *wavelet_host,
+                    int64_t nt, void *traces_host)
+{
+    if (!cfg || !labels_host || !medium || !probe || (nt > 0 && !traces_host))
+        return fail(PE_ERR_INVALID, "null argument");
+    const long long ncell = (long long)cfg->nz * cfg->ny * cfg->nx;
+    if (ncell <= 0) return fail(PE_ERR_INVALID, "grid dimensions must be positive");
+    const int es = dtype_size(cfg->dtype);
+    uint16_t *lab = nullptr;
+    float *dvol = nullptr;
+    void *fields = nullptr, *traces = nullptr;
+    PeSolver *S = nullptr;
+    int rc = PE_OK;
+    cudaStream_t st = nullptr;
+    PeMedium md = *medium;
+    PeState state{};
+    const size_t tr_bytes = (size_t)es * (size_t)std::max<int64_t>(1, nt) * std::max(1, probe->n_groups);
+    do {
+        if ((rc = dev_alloc(&lab, sizeof(uint16_t) * ncell))) break;
+        if (damp_host && (rc = dev_alloc(&dvol, sizeof(float) * ncell))) break;
+        if ((rc = dev_alloc(&fields, (size_t)es * 9 * ncell))) break;
+        if ((rc = dev_alloc(&traces, tr_bytes))) break;
+        cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(lab, labels_host, sizeof(uint16_t) * ncell, cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess && dvol)
+            ce = cudaMemcpyAsync(dvol, damp_host, sizeof(float) * ncell, cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(fields, 0, (size_t)es * 9 * ncell, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) {
+            rc = fail(PE_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce));
+            break;
+        }
+        md.labels_dev = lab;
+        md.damp_volume_dev = dvol;
+        if ((rc = pe_solver_create(cfg, &md, probe, &S))) break;
+        if ((rc = pe_solver_set_wavelet(S, wavelet_host, nt))) break;
+        for (int i = 0; i < 3; ++i) state.v[i] = (char *)fields + (size_t)es * i * ncell;
+        for (int i = 0; i < 6; ++i) state.s[i] = (char *)fields + (size_t)es * (3 + i) * ncell;
+        if ((rc = pe_solver_run(S, &state, traces, 0, nt, st))) break;
+        if (probe->n_groups > 0 && nt > 0) {
+            ce = cudaMemcpyAsync(traces_host, traces, (size_t)es * nt * probe->n_groups, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            if (ce != cudaSuccess) {
+                rc = fail(PE_ERR_CUDA, std::string("download: ") + cudaGetErrorString(ce));
+                break;
+            }
+        }
+    } while (0);
+    if (S) pe_solver_destroy(S);
+    if (st) cudaStreamSynchronize(st), cudaStreamDestroy(st);
+    if (lab) cudaFree(lab);
+    if (dvol) cudaFree(dvol);
+    if (fields) cudaFree(fields);
+    if (traces) cudaFree(traces);
+    return rc;
+}
+
+}  // extern "C"

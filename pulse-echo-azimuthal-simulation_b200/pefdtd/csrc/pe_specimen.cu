@@ -1,0 +1,98 @@
+// Power-diagram (Laguerre) labelling of a cylinder on the device.
+//
+// Same arithmetic as the reference's exact labeller
+// (sim/core/specimen.py:298-337): per grid point, in float64,
+//   d = ((x - sx)^2 + (y - sy)^2) - w  +  (z - sz)^2
+// minimised over ALL seeds, first index on ties, -1 where x^2 + y^2 > R2
+// (R2 is the caller's R**2, so the inside test matches bit for bit).
+// Compiled with -fmad=false so no product is fused into a sum, as in NumPy.
+// One thread per cell; seeds are staged through shared memory in tiles.
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "pefdtd.h"
+
+namespace {
+
+constexpr int SEED_TILE = 256;
+
+__global__ void k_label_cylinder(const double *__restrict__ xs, const double *__restrict__ ys,
+                                 const double *__restrict__ zs, int nx, int ny, int nz, double R2,
+                                 const double *__restrict__ seeds, const double *__restrict__ w,
+                                 int ns, int32_t *__restrict__ out)
+{
+    __shared__ double sh[SEED_TILE][4];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)nx * ny * nz;
+    const bool live = i < n;
+    int ix = 0, iy = 0, iz = 0;
+    if (live) {
+        ix = (int)(i % nx);
+        iy = (int)((i / nx) % ny);
+        iz = (int)(i / ((long long)nx * ny));
+    }
+    const double x = live ? xs[ix] : 0.0, y = live ? ys[iy] : 0.0, z = live ? zs[iz] : 0.0;
+    const bool inside = live && (x * x + y * y <= R2);
+    double best = 0.0;
+    int arg = -1;
+    for (int t0 = 0; t0 < ns; t0 += SEED_TILE) {
+        const int nt = min(SEED_TILE, ns - t0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nt; k += blockDim.x) {
+            sh[k][0] = seeds[(t0 + k) * 3 + 0];
+            sh[k][1] = seeds[(t0 + k) * 3 + 1];
+            sh[k][2] = seeds[(t0 + k) * 3 + 2];
+            sh[k][3] = w[t0 + k];
+        }
+        __syncthreads();
+        if (inside) {
+            for (int k = 0; k < nt; ++k) {
+                const double dx = x - sh[k][0], dy = y - sh[k][1], dz = z - sh[k][2];
+                double d = dx * dx + dy * dy;
+                d = d - sh[k][3];
+                d = d + dz * dz;
+                if (arg < 0 || d < best) {
+                    best = d;
+                    arg = t0 + k;
+                }
+            }
+        }
+    }
+    if (live) out[i] = inside ? arg : -1;
+}
+
+thread_local std::string g_err_spec;
+
+}  // namespace
+
+extern "C" int pe_label_cylinder(const double *xs, int nx, const double *ys, int ny,
+                                 const double *zs, int nz, double R2, const double *seeds,
+                                 const double *weights, int ns, int32_t *out_dev, void *stream)
+{
+    if (!xs || !ys || !zs || !seeds || !out_dev || nx < 1 || ny < 1 || nz < 1 || ns < 1)
+        return PE_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *d = nullptr;
+    const size_t nb = sizeof(double) * ((size_t)nx + ny + nz + 4 * (size_t)ns);
+    if (cudaMalloc(&d, nb) != cudaSuccess) return PE_ERR_NOMEM;
+    double *dx = d, *dy = dx + nx, *dz = dy + ny, *ds = dz + nz, *dw = ds + 3 * (size_t)ns;
+    cudaError_t e = cudaMemcpyAsync(dx, xs, sizeof(double) * nx, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dy, ys, sizeof(double) * ny, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, zs, sizeof(double) * nz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, seeds, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        if (weights) e = cudaMemcpyAsync(dw, weights, sizeof(double) * ns, cudaMemcpyHostToDevice, st);
+        else e = cudaMemsetAsync(dw, 0, sizeof(double) * ns, st);
+    }
+    if (e == cudaSuccess) {
+        const long long n = (long long)nx * ny * nz;
+        k_label_cylinder<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dx, dy, dz, nx, ny, nz, R2, ds,
+                                                                     dw, ns, out_dev);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    return e == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+}

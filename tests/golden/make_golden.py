@@ -1,0 +1,145 @@
+"""Generate the golden fixtures in tests/golden/ by importing the reference.
+
+Run where the reference tree is present (default /root/reference, override
+with PE_REFERENCE_ROOT):  python tests/golden/make_golden.py
+
+Every fixture records what the reference itself computes for seeded inputs
+(the inputs are stored beside the outputs, so the tests need no reference at
+run time):
+  coeffs.json        optimised_coeffs / taylor_coeffs / cfl_limit
+  tables.npz         material_tables for seeded c-axes; safe_dt_labels
+  sponge.npz         sponge_profile volumes; face_density
+  wavelets.npz       ricker, hann_tone_burst, pick_peak on a seeded trace
+  specimen.npz       DiskSpecimen.build (CPU labeller), build_grid and
+                     rotated_grid at two azimuths, sample_watson
+  forward_small.npz  fdtd.forward traces (FP64 on CPU, and FP32 through a
+                     NumPy stand-in for CuPy) for a small seeded disk, both
+                     records, with the inputs that produced them
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("PE_REFERENCE_ROOT", "/root/reference")
+sys.path[:0] = [os.path.join(REF, "sim", "core"), os.path.join(REF, "vendor"),
+                os.path.join(REF, "sim", "fw_checks")]
+
+
+def _numpy_as_cupy():
+    """A module that answers to `import cupy` with NumPy, so the reference's
+    array path runs its float32 branch on the CPU."""
+    m = types.ModuleType("cupy")
+    m.__getattr__ = lambda name: getattr(np, name)
+    m.asnumpy = np.asarray
+    rt = types.SimpleNamespace(getDeviceCount=lambda: 1)
+    m.cuda = types.SimpleNamespace(runtime=rt)
+    return m
+
+
+def main():
+    import fdtd
+    from ringfwi import anisotropy as an
+    from ringfwi import sources
+    import specimen as spm
+
+    out = {}
+    # ---- coefficients
+    co = {}
+    for order in (2, 4, 6, 8):
+        co[f"taylor_{order}"] = list(map(float, fdtd.taylor_coeffs(order)))
+    for kh, ms in ((1.6, True), (2.0, True), (1.6, False)):
+        co[f"opt_8_{kh}_{ms}"] = list(map(float, fdtd.optimised_coeffs(8, kh_max=kh, multistart=ms)))
+    co["opt_4_1.6_True"] = list(map(float, fdtd.optimised_coeffs(4)))
+    co["opt_6_1.6_True"] = list(map(float, fdtd.optimised_coeffs(6)))
+    co["cfl_8_2.0"] = float(fdtd.cfl_limit(np.array(co["opt_8_2.0_True"])))
+    with open(os.path.join(HERE, "coeffs.json"), "w") as f:
+        json.dump(co, f, indent=1)
+
+    # ---- material tables
+    rng = np.random.default_rng(11)
+    axes = rng.normal(size=(300, 3))
+    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+    axes[0] = [0, 0, 1]
+    axes[1] = [0, 0, -1]
+    axes[2] = [1, 0, 0]
+    Ct, rho_t = fdtd.material_tables(axes)
+    Ct2, rho2 = fdtd.material_tables(axes[:20], c_couplant=1480.0, rho_couplant=1000.0)
+    lab = rng.integers(-1, 20, size=(10, 12, 14))
+    mats = (lab + 1).astype(np.uint8)
+    dt_lab = fdtd.safe_dt_labels(mats, Ct, rho_t, 1e-4, np.array(co["opt_8_2.0_True"]), safety=0.5)
+    np.savez_compressed(os.path.join(HERE, "tables.npz"), axes=axes, Ct=Ct, rho_t=rho_t,
+                        Ct2=Ct2, rho2=rho2, lab=lab, dt_lab=dt_lab)
+
+    # ---- sponge / face density
+    sp1 = fdtd.sponge_profile((20, 24, 30), 6)
+    sp2 = fdtd.sponge_profile((9, 40, 7), 5, strength=0.2)
+    rho_cell = rng.uniform(300, 917, size=(6, 7, 8))
+    fd = np.stack([fdtd.face_density(rho_cell, a) for a in range(3)])
+    np.savez_compressed(os.path.join(HERE, "sponge.npz"), sp1=sp1, sp2=sp2, rho_cell=rho_cell, fd=fd)
+
+    # ---- wavelets and picks
+    dtw = 2e-8
+    rk = fdtd.ricker(2e6, dtw, 800)
+    hb = sources.hann_tone_burst(800, dtw, 1e6, n_cycles=3)
+    t = np.arange(3000) * dtw
+    tr = (np.exp(-((t - 20e-6) / 1e-6) ** 2) * np.sin(2 * np.pi * 2e6 * t)
+          + 0.01 * rng.standard_normal(3000))
+    pk = fdtd.pick_peak(t, tr, t_lo=10e-6, t_hi=40e-6, dt=dtw)
+    pk_hp = fdtd.pick_peak(t, tr, t_lo=10e-6, t_hi=40e-6, dt=dtw, f_lo=0.3e6)
+    np.savez_compressed(os.path.join(HERE, "wavelets.npz"), ricker=rk, hann=hb, t=t, tr=tr,
+                        pick=np.array(pk[:2]), pick_ok=pk[2], pick_hp=np.array(pk_hp[:2]))
+
+    # ---- specimen (CPU labeller: CuPy absent), grid builders, Watson
+    sp = spm.DiskSpecimen(diameter_m=0.012, thickness_m=0.006, n_grains=25, size_cv=0.35,
+                          concentration=3.0, spatial_corr=0.0, fabric_axis=(1, 0, 0), seed=7)
+    b = sp.build(0.5e-3)
+    import coda_convergence as CC
+    import rotation_test as RT
+    g_lab, nd, m = CC.build_grid(b, 0.4e-3, 4)
+    r_lab17, _, _, r_ax17 = RT.rotated_grid(b, 0.4e-3, 4, 17)
+    r_lab90, _, _, r_ax90 = RT.rotated_grid(b, 0.4e-3, 4, 90)
+    w_rng = np.random.default_rng(3)
+    wat = spm.sample_watson(200, (1.0, 0.0, 1.0), 5.0, w_rng)
+    wat_g = spm.sample_watson(100, (0.0, 0.0, 1.0), -4.0, w_rng)
+    seeds_rng = np.random.default_rng(21)
+    seeds = spm.DiskSpecimen._seed_points(5e-3, 3e-3, 40, seeds_rng)
+    np.savez_compressed(os.path.join(HERE, "specimen.npz"), labels=b["labels"], axes=b["axes"],
+                        seeds=b["seeds"], weights=b["weights"], h=b["h"], grid_lab=g_lab,
+                        rot17=r_lab17, rot17_axes=r_ax17, rot90=r_lab90, rot90_axes=r_ax90,
+                        watson=wat, watson_girdle=wat_g, seed_pts=seeds)
+
+    # ---- forward traces on a small seeded disk
+    sys.path.insert(0, os.path.dirname(HERE))
+    from helpers import make_small
+    p = make_small(nt=160, shape=(22, 26, 30), n_grains=10, sponge=4)
+    lab = p["lab"]
+    C, rho = an.polycrystal_stiffness_3d(lab, p["axes"], c_couplant=1500.0, rho_couplant=300.0)
+    res = dict(lab=lab.astype(np.int16), axes=p["axes"], h=p["h"], dt=p["dt"], nt=p["nt"],
+               coeffs=p["coeffs"], wavelet=p["wavelet"], sponge=p["sponge"],
+               src=np.array([q for q, _ in p["src_pts"]]), w=p["src_pts"][0][1])
+    recs = p["rec_groups"]
+    for record in ("pressure", "vz"):
+        tr64 = fdtd.forward(C, rho, p["h"], p["dt"], p["nt"], p["src_pts"], p["wavelet"], recs,
+                            coeffs=p["coeffs"], sponge_width=p["sponge"], device="cpu",
+                            record=record)
+        sys.modules["cupy"] = _numpy_as_cupy()
+        try:
+            tr32 = fdtd.forward(C, rho, p["h"], p["dt"], p["nt"], p["src_pts"], p["wavelet"],
+                                recs, coeffs=p["coeffs"], sponge_width=p["sponge"], device="gpu",
+                                record=record)
+        finally:
+            del sys.modules["cupy"]
+        res[f"{record}_f64"] = tr64
+        res[f"{record}_f32"] = tr32
+    np.savez_compressed(os.path.join(HERE, "forward_small.npz"), **res)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,214 @@
+"""GPU parity of the CUDA solver (calls go through the C ABI).
+
+Bar: bit-exact against the CPU oracle with the product's FMA placement
+(fma_mode 1) in FP32 and FP64; relative L2 <= 1e-5 against the reference's
+own update kernels (oracle/_ref, every product rounded separately) and the
+reference NumPy array path (golden); identical echo picks.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import make_small, oracle_prob, rel_l2
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5   # FP32 trace rel-L2 against the reference's own update
+
+
+def _fwd(p, **kw):
+    from pefdtd import fdtd
+    kw.setdefault("coeffs", p["coeffs"])
+    kw.setdefault("sponge_width", p["sponge"])
+    return fdtd.forward_fused_labels(p["lab"], p["axes"], p["h"], p["dt"], p["nt"], p["src_pts"],
+                                     p["wavelet"], p["rec_groups"], **kw)
+
+
+@pytest.mark.parametrize("record", ["pressure", "vz", "vx", "vy"])
+@pytest.mark.parametrize("damped", [False, True])
+def test_bit_exact_vs_oracle_f32(record, damped):
+    p = make_small(nt=150, shape=(22, 26, 30), n_grains=10, sponge=4)
+    tr = _fwd(p, record=record, damped_record=damped)
+    ref = O.run_oracle(oracle_prob(p, record=record, damped_record=damped), fma_mode=1)
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(tr, ref), f"max |diff| {np.abs(tr - ref).max()}"
+
+
+def test_bit_exact_vs_oracle_f64_and_f32_error():
+    p = make_small(nt=150, shape=(22, 26, 30), n_grains=10, sponge=4)
+    from pefdtd.fdtd import _material_tables64
+    Ct, rho = _material_tables64(p["axes"], 1500.0, 300.0)
+    tr64 = _fwd(p, record="pressure", damped_record=True, dtype="float64")
+    ref64 = O.run_oracle(oracle_prob(p, record="pressure", dtype=np.float64, Ct=Ct, rho_t=rho),
+                         dtype=np.float64, fma_mode=1)
+    assert tr64.dtype == np.float64
+    assert np.array_equal(tr64, ref64)
+    tr32 = _fwd(p, record="pressure", damped_record=True)
+    assert rel_l2(tr32, tr64) < 1e-5
+
+
+@pytest.mark.parametrize("shape,tile,zc,chunk", [
+    ((17, 23, 19), (32, 8), 0, 0),
+    ((33, 41, 37), (32, 4), 7, 13),
+    ((24, 70, 66), (32, 8), 5, 200),
+    ((40, 9, 100), (32, 4), 40, 1),
+])
+def test_odd_grids_tiles_and_schedules(shape, tile, zc, chunk):
+    p = make_small(nt=60, shape=shape, n_grains=7, sponge=2)
+    from pefdtd import damping
+    mask = damping.fluid_damp_mask(p["lab"], 0.05)
+    tr = _fwd(p, record="pressure", damp_mask=mask, damped_record=True, tile=tile, z_chunk=zc,
+              chunk_steps=chunk)
+    ref = O.run_oracle(oracle_prob(p, record="pressure", damped_record=True, damp_mask=mask),
+                       fma_mode=1)
+    assert np.array_equal(tr, ref)
+
+
+def test_vs_reference_own_kernels_rel_l2():
+    if O.ref_lib() is None:
+        pytest.skip("reference harness not built")
+    p = make_small(nt=400, shape=(28, 34, 36), n_grains=14, sponge=4)
+    for record in ("pressure", "vz"):
+        tr = _fwd(p, record=record)
+        ref = O.run_reference_labels(oracle_prob(p, record=record, damped_record=False))
+        assert rel_l2(tr, ref) < TOL
+
+
+def test_many_materials_vs_reference_dense():
+    if O.ref_lib() is None:
+        pytest.skip("reference harness not built")
+    p = make_small(nt=120, shape=(20, 34, 34), n_grains=400, sponge=3)
+    assert p["n_grains"] > 255
+    tr = _fwd(p, record="vz", damped_record=True)
+    pr = oracle_prob(p, record="vz", damped_record=True)
+    assert np.array_equal(tr, O.run_oracle(pr, fma_mode=1))
+    assert rel_l2(tr, O.run_reference_dense(pr)) < TOL
+
+
+def test_disk_small_workload_parity_and_picks():
+    """The benchmark's small configuration (64 x 96 x 96, 50 grains), 600
+    steps: bit-exact vs the oracle, within 1e-5 of the reference kernels,
+    same echo pick."""
+    from pefdtd import workloads, wavelets
+    p = workloads.make_problem("disk_small", nt=600)
+    tr = _fwd(p, record="vz", damped_record=True)
+    pr = oracle_prob(p, record="vz", damped_record=True)
+    assert np.array_equal(tr, O.run_oracle(pr, fma_mode=1))
+    if O.ref_lib() is not None:
+        ref = O.run_reference_labels(pr) if p["mats"].max() < 256 else O.run_reference_dense(pr)
+        # the label-path harness records pre-damp stress but vz is identical
+        assert rel_l2(tr, ref) < TOL
+        t = np.arange(p["nt"]) * p["dt"]
+        a = wavelets.pick_peak(t, tr.ravel(), t_lo=t[len(t) // 5], dt=p["dt"])
+        b = wavelets.pick_peak(t, ref.ravel(), t_lo=t[len(t) // 5], dt=p["dt"])
+        assert np.isfinite(a[0]) and a[2] == b[2]
+        assert abs(a[0] - b[0]) < 1e-3 * p["dt"]
+
+
+def test_golden_numpy_path_and_drop_in_forward():
+    from pefdtd import fdtd
+    from pefdtd.materials import stiffness_maps
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "forward_small.npz"))
+    lab = g["lab"].astype(np.int32)
+    pts = [tuple(q) for q in g["src"]]
+    w = float(g["w"])
+    C, rho = stiffness_maps(lab, g["axes"])
+    for record in ("pressure", "vz"):
+        tr = fdtd.forward(C, rho, float(g["h"]), float(g["dt"]), int(g["nt"]), [(q, w) for q in pts],
+                          g["wavelet"], [(pts, np.full(len(pts), w))], coeffs=g["coeffs"],
+                          sponge_width=int(g["sponge"]), device="gpu", record=record)
+        assert rel_l2(tr.ravel(), g[f"{record}_f32"].ravel()) < TOL
+        assert rel_l2(tr.ravel(), g[f"{record}_f64"].ravel()) < TOL
+        tr64 = fdtd.forward(C, rho, float(g["h"]), float(g["dt"]), int(g["nt"]), [(q, w) for q in pts],
+                            g["wavelet"], [(pts, np.full(len(pts), w))], coeffs=g["coeffs"],
+                            sponge_width=int(g["sponge"]), device="cpu", record=record)
+        assert rel_l2(tr64.ravel(), g[f"{record}_f64"].ravel()) < 1e-9
+
+
+def test_errors_match_reference_behaviour():
+    from pefdtd import fdtd
+    p = make_small(nt=20, shape=(16, 20, 20), n_grains=5, sponge=2)
+    with pytest.raises(ValueError, match="order <= 8"):
+        _fwd(p, coeffs=[1.0, 0.1, 0.01, 0.001, 0.0001])
+    bad = p["lab"].copy()
+    bad[0, 0, 0] = -2
+    with pytest.raises(ValueError, match="labels must lie"):
+        fdtd.forward_fused_labels(bad, p["axes"], p["h"], p["dt"], p["nt"], p["src_pts"],
+                                  p["wavelet"], p["rec_groups"], coeffs=p["coeffs"])
+    with pytest.raises(ValueError, match="has no c-axis"):
+        fdtd.forward_fused_labels(p["lab"], p["axes"][:2], p["h"], p["dt"], p["nt"], p["src_pts"],
+                                  p["wavelet"], p["rec_groups"], coeffs=p["coeffs"])
+    # a probe inside the sponge is refused unless the damped convention is asked for
+    src = [((1, 10, 10), 1.0)]
+    with pytest.raises(ValueError, match="damp < 0.999"):
+        fdtd.forward_fused_labels(p["lab"], p["axes"], p["h"], p["dt"], p["nt"], src, p["wavelet"],
+                                  [([(1, 10, 10)], [1.0])], coeffs=p["coeffs"], sponge_width=4)
+    out = fdtd.forward_fused_labels(p["lab"], p["axes"], p["h"], p["dt"], p["nt"], src, p["wavelet"],
+                                    [([(1, 10, 10)], [1.0])], coeffs=p["coeffs"], sponge_width=4,
+                                    damped_record=True)
+    assert out.shape == (p["nt"], 1)
+
+
+def test_progress_callback_cadence_and_abort():
+    p = make_small(nt=450, shape=(16, 20, 20), n_grains=5, sponge=2)
+    seen = []
+    _fwd(p, progress=lambda f: seen.append(f))
+    assert seen == [0.0, 200 / 450, 400 / 450]
+
+    class Stop(Exception):
+        pass
+
+    def stop(f):
+        if f > 0:
+            raise Stop()
+    with pytest.raises(Stop):
+        _fwd(p, progress=stop)
+
+
+def test_host_entry_matches_device_path():
+    """pe_forward_host (host buffers in and out) == DeviceSolve traces."""
+    import ctypes as C
+    from pefdtd import _capi
+    from pefdtd.damping import sponge_axis_profiles
+    from pefdtd.fdtd import _flat_probe
+    p = make_small(nt=90, shape=(20, 24, 28), n_grains=8, sponge=3)
+    shape = p["lab"].shape
+    s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float32)
+    cfg = _capi.PeConfig()
+    cfg.nz, cfg.ny, cfg.nx = shape
+    cfg.dtype = _capi.PE_F32
+    cfg.n_coeffs = len(p["coeffs"])
+    for j, c in enumerate(p["coeffs"]):
+        cfg.coeffs[j] = float(c)
+    cfg.h, cfg.dt = p["h"], p["dt"]
+    cfg.record, cfg.damped_record, cfg.n_mat = 0, 1, len(p["rho_t"])
+    Ct = np.ascontiguousarray(p["Ct"], np.float32)
+    rho = np.ascontiguousarray(p["rho_t"], np.float32)
+    sp = [np.ascontiguousarray(a) for a in sponge_axis_profiles(shape, p["sponge"])]
+    md = _capi.PeMedium()
+    md.ctab, md.rho = _capi.ptr(Ct), _capi.ptr(rho)
+    md.sponge_z, md.sponge_y, md.sponge_x = [_capi.ptr(a) for a in sp]
+    pr = _capi.PeProbe()
+    pr.n_src, pr.src_idx, pr.src_w = len(s_idx), _capi.ptr(s_idx), _capi.ptr(s_w)
+    pr.n_groups, pr.rec_off, pr.rec_idx, pr.rec_w = 1, _capi.ptr(r_off), _capi.ptr(r_idx), _capi.ptr(r_w)
+    labs = np.ascontiguousarray(p["mats"], np.uint16)
+    wav = np.ascontiguousarray(p["wavelet"], np.float32)
+    out = np.zeros((p["nt"], 1), np.float32)
+    _capi.check(_capi.lib().pe_forward_host(C.byref(cfg), _capi.ptr(labs), None, C.byref(md),
+                                            C.byref(pr), _capi.ptr(wav), p["nt"], _capi.ptr(out)))
+    ref = O.run_oracle(oracle_prob(p, record="pressure", damped_record=True), fma_mode=1)
+    assert np.array_equal(out, ref)
+
+
+def test_gpu_labeller_bit_exact():
+    from pefdtd import specimen
+    rng = np.random.default_rng(4)
+    seeds = specimen.seed_points(5e-3, 3e-3, 60, rng)
+    w = rng.uniform(0, 2e-7, 60)
+    x = (np.arange(50) - 24.5) * 0.2e-3
+    z = (np.arange(16) - 7.5) * 0.2e-3
+    for ww in (None, w):
+        a = specimen.label_cylinder(x, x[:44], z, 5e-3, seeds, ww).cpu().numpy()
+        b = specimen.label_cylinder_numpy(x, x[:44], z, 5e-3, seeds, ww)
+        assert np.array_equal(a, b)
