@@ -66,9 +66,14 @@ typedef struct PeConfig {
                                forward_fused / forward (:909-915, :361-367) */
     int32_t n_mat;          /* rows in the material tables, 1..PE_MAX_MATERIALS */
     int32_t chunk_steps;    /* steps per captured CUDA graph (0 = 200) */
-    int32_t tile_x, tile_y; /* kernel tile (0 = tuned default) */
+    int32_t tile_x, tile_y; /* simple-kernel tile (0 = default) */
     int32_t z_chunk;        /* planes per z-march (0 = tuned default) */
+    int32_t variant;        /* PeKernelVariant (0 = tiled, the default) */
 } PeConfig;
+
+/* Kernel family. Both are bit-identical; SIMPLE reads every tap through the
+ * L1 cache and is kept as an independent cross-check of TILED. */
+enum PeKernelVariant { PE_KERNEL_TILED = 0, PE_KERNEL_SIMPLE = 1 };
 
 /* The medium. Volumes live on the device; tables are small host arrays. */
 typedef struct PeMedium {

@@ -23,7 +23,11 @@ class PeConfig(C.Structure):
                 ("coeffs", C.c_double * 4), ("h", C.c_double), ("dt", C.c_double),
                 ("record", C.c_int32), ("damped_record", C.c_int32),
                 ("n_mat", C.c_int32), ("chunk_steps", C.c_int32),
-                ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("z_chunk", C.c_int32)]
+                ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("z_chunk", C.c_int32),
+                ("variant", C.c_int32)]
+
+
+KERNEL_VARIANT = {"tiled": 0, "simple": 1}
 
 
 class PeMedium(C.Structure):

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "pe_kernels.cuh"
+#include "pe_kernels_tiled.cuh"
 #include "pefdtd.h"
 
 namespace {
@@ -84,7 +85,9 @@ struct PeSolver {
     PeState gstate{};
     void *gtraces = nullptr;
     int chunk = 200;
-    int tx = 32, ty = 8, zc = 0;
+    int tx = 32, ty = 8;        // simple-kernel tile
+    int variant = PE_KERNEL_TILED;
+    int zc_s = 0, zc_v = 0;     // planes per z-march of the stress / velocity launches
     long long launches = 0;
 
     ~PeSolver()
@@ -137,17 +140,55 @@ pe::StepArgs<T> make_args(const PeSolver *S, const PeState *st, int k)
     A.rec_damped = S->cfg.damped_record;
     A.step = S->step;
     A.k = k;
-    A.zc = S->zc;
+    A.zc = S->zc_s;
     return A;
 }
 
 template <typename T, int TX, int TY>
-void launch_pair(const pe::StepArgs<T> &A, cudaStream_t st)
+void launch_simple_stress(pe::StepArgs<T> A, int zc, cudaStream_t st)
 {
-    dim3 block(TX, TY, 1);
-    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + A.zc - 1) / A.zc);
-    pe::k_stress<T, TX, TY><<<grid, block, 0, st>>>(A);
-    pe::k_velocity<T, TX, TY><<<grid, block, 0, st>>>(A);
+    A.zc = zc;
+    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + zc - 1) / zc);
+    pe::k_stress<T, TX, TY><<<grid, dim3(TX, TY, 1), 0, st>>>(A);
+}
+template <typename T, int TX, int TY>
+void launch_simple_velocity(pe::StepArgs<T> A, int zc, cudaStream_t st)
+{
+    A.zc = zc;
+    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + zc - 1) / zc);
+    pe::k_velocity<T, TX, TY><<<grid, dim3(TX, TY, 1), 0, st>>>(A);
+}
+
+template <typename T>
+void launch_stress(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st)
+{
+    if (S->variant == PE_KERNEL_SIMPLE) {
+        if (S->ty == 8) launch_simple_stress<T, 32, 8>(A0, S->zc_s, st);
+        else launch_simple_stress<T, 32, 4>(A0, S->zc_s, st);
+        return;
+    }
+    pe::StepArgs<T> A = A0;
+    A.zc = S->zc_s;
+    dim3 grid((A.nx + pe::TS_OX - 1) / pe::TS_OX, (A.ny + pe::TS_OY - 1) / pe::TS_OY,
+              (A.nz + A.zc - 1) / A.zc);
+    pe::k_stress_t<T><<<grid, dim3(pe::TB_X, pe::TB_Y, 1), pe::stress_tiled_smem<T>(S->cfg.n_mat), st>>>(
+        A, S->cfg.n_mat);
+}
+
+template <typename T>
+void launch_velocity(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st)
+{
+    if (S->variant == PE_KERNEL_SIMPLE) {
+        if (S->ty == 8) launch_simple_velocity<T, 32, 8>(A0, S->zc_v, st);
+        else launch_simple_velocity<T, 32, 4>(A0, S->zc_v, st);
+        return;
+    }
+    pe::StepArgs<T> A = A0;
+    A.zc = S->zc_v;
+    dim3 grid((A.nx + pe::TB_X - 1) / pe::TB_X, (A.ny + pe::TB_Y - 1) / pe::TB_Y,
+              (A.nz + A.zc - 1) / A.zc);
+    pe::k_velocity_t<T><<<grid, dim3(pe::TB_X, pe::TB_Y, 1), pe::velocity_tiled_smem<T>(S->cfg.n_mat),
+                          st>>>(A, S->cfg.n_mat);
 }
 
 template <typename T>
@@ -155,8 +196,8 @@ int launch_chunk_t(PeSolver *S, const PeState *st, void *traces, int len)
 {
     for (int k = 0; k < len; ++k) {
         pe::StepArgs<T> A = make_args<T>(S, st, k);
-        if (S->tx == 32 && S->ty == 8) launch_pair<T, 32, 8>(A, S->stream);
-        else launch_pair<T, 32, 4>(A, S->stream);
+        launch_stress<T>(S, A, S->stream);
+        launch_velocity<T>(S, A, S->stream);
         S->launches += 2;
     }
     if (S->n_groups > 0) {
@@ -187,21 +228,68 @@ bool same_state(const PeState &a, const PeState &b)
     return true;
 }
 
-int pick_zchunk(const PeSolver *S)
+// Planes per z-march: the split of nz into chunks that minimises
+// waves x (planes per chunk + per-chunk start-up planes), where a wave is
+// one block on every SM slot the occupancy allows.
+int pick_zchunk(int nz, long long tiles, int slots, int startup)
 {
-    if (S->cfg.z_chunk > 0) return S->cfg.z_chunk;
-    // enough blocks to give every SM several, without short marches
-    int dev = 0, nsm = 148;
+    int best_zc = nz;
+    double best = 1e300;
+    for (int nch = 1; nch <= nz; ++nch) {
+        const int zc = (nz + nch - 1) / nch;
+        const int real = (nz + zc - 1) / zc;
+        if (zc < 4 && nch > 1) break;
+        const long long blocks = tiles * real;
+        const long long waves = (blocks + slots - 1) / slots;
+        const double cost = (double)waves * (zc + startup);
+        if (cost < best - 1e-9) {
+            best = cost;
+            best_zc = zc;
+        }
+    }
+    return best_zc;
+}
+
+template <typename K>
+int occupancy_slots(K kernel, int threads, size_t smem)
+{
+    int dev = 0, nsm = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const long long tiles = (long long)((S->cfg.nx + S->tx - 1) / S->tx) *
-                            ((S->cfg.ny + S->ty - 1) / S->ty);
-    const long long want = 4LL * nsm;
-    long long nchunks = (want + tiles - 1) / tiles;
-    int zc = (int)((S->cfg.nz + nchunks - 1) / nchunks);
-    if (zc < 16) zc = 16;
-    if (zc > S->cfg.nz) zc = S->cfg.nz;
-    return zc;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1)
+        per = 1;
+    return nsm * per;
+}
+
+template <typename T>
+int configure_kernels(PeSolver *S)
+{
+    const PeConfig &c = S->cfg;
+    if (S->variant == PE_KERNEL_SIMPLE) {
+        const long long tiles = (long long)((c.nx + S->tx - 1) / S->tx) * ((c.ny + S->ty - 1) / S->ty);
+        const int slots = occupancy_slots(pe::k_stress<T, 32, 8>, 32 * S->ty, 0);
+        S->zc_s = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tiles, slots, 2);
+        S->zc_v = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tiles, slots, 2);
+        return PE_OK;
+    }
+    // allow every launch up to the device's opt-in shared memory per block
+    int dev = 0, optin = 0;
+    PE_CUDA(cudaGetDevice(&dev));
+    PE_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t need_s = pe::stress_tiled_smem<T>(c.n_mat), need_v = pe::velocity_tiled_smem<T>(c.n_mat);
+    if (need_s > (size_t)optin || need_v > (size_t)optin)
+        return fail(PE_ERR_UNSUPPORTED, "tiled kernels need " + std::to_string(need_s) +
+                                            " B of shared memory per block; device offers " +
+                                            std::to_string(optin));
+    PE_CUDA(cudaFuncSetAttribute(pe::k_stress_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    const long long ts = (long long)((c.nx + pe::TS_OX - 1) / pe::TS_OX) * ((c.ny + pe::TS_OY - 1) / pe::TS_OY);
+    const long long tv = (long long)((c.nx + pe::TB_X - 1) / pe::TB_X) * ((c.ny + pe::TB_Y - 1) / pe::TB_Y);
+    const int ss = occupancy_slots(pe::k_stress_t<T>, pe::TB_X * pe::TB_Y, need_s);
+    const int sv = occupancy_slots(pe::k_velocity_t<T>, pe::TB_X * pe::TB_Y, need_v);
+    S->zc_s = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, ts, ss, 4);
+    S->zc_v = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tv, sv, 3);
+    return PE_OK;
 }
 
 }  // namespace
@@ -219,6 +307,8 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     const PeConfig &c = *cfg;
     if (c.nz < 1 || c.ny < 1 || c.nx < 1)
         return fail(PE_ERR_INVALID, "grid dimensions must be positive");
+    if ((long long)c.ny * c.nx >= (1LL << 31))
+        return fail(PE_ERR_UNSUPPORTED, "an xy plane must hold fewer than 2^31 cells");
     if (c.n_coeffs < 1 || c.n_coeffs > 4)
         return fail(PE_ERR_INVALID,
                     "supports order <= 8 (" + std::to_string(c.n_coeffs) +
@@ -243,15 +333,22 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     S->ncell = (long long)c.nz * c.ny * c.nx;
     S->esize = dtype_size(c.dtype);
     S->chunk = c.chunk_steps > 0 ? c.chunk_steps : 200;
+    if (c.variant != PE_KERNEL_TILED && c.variant != PE_KERNEL_SIMPLE)
+        return fail(PE_ERR_INVALID, "variant must be PE_KERNEL_TILED or PE_KERNEL_SIMPLE");
+    S->variant = c.variant;
     if (c.tile_x > 0 && c.tile_y > 0) {
         const TileShape ok[] = {{32, 8}, {32, 4}};
         bool found = false;
         for (auto t : ok) found |= (t.tx == c.tile_x && t.ty == c.tile_y);
-        if (!found) return fail(PE_ERR_UNSUPPORTED, "tile shape not compiled in");
+        if (!found || S->variant != PE_KERNEL_SIMPLE)
+            return fail(PE_ERR_UNSUPPORTED, "tile shape not compiled in for this kernel variant");
         S->tx = c.tile_x;
         S->ty = c.tile_y;
     }
-    S->zc = pick_zchunk(S.get());
+    {
+        int rc0 = c.dtype == PE_F64 ? configure_kernels<double>(S.get()) : configure_kernels<float>(S.get());
+        if (rc0) return rc0;
+    }
     const long long ncell = S->ncell;
     const int es = S->esize;
 
@@ -469,20 +566,14 @@ int pe_solver_profile(PeSolver *S, const PeState *state, int n_steps, float *ms_
         PE_CUDA(cudaEventRecord(ev[0], S->stream));
         if (S->cfg.dtype == PE_F64) {
             pe::StepArgs<double> A = make_args<double>(S, state, 0);
-            dim3 grid((A.nx + S->tx - 1) / S->tx, (A.ny + S->ty - 1) / S->ty, (A.nz + A.zc - 1) / A.zc);
-            if (S->ty == 8) pe::k_stress<double, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
-            else pe::k_stress<double, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+            launch_stress<double>(S, A, S->stream);
             PE_CUDA(cudaEventRecord(ev[1], S->stream));
-            if (S->ty == 8) pe::k_velocity<double, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
-            else pe::k_velocity<double, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+            launch_velocity<double>(S, A, S->stream);
         } else {
             pe::StepArgs<float> A = make_args<float>(S, state, 0);
-            dim3 grid((A.nx + S->tx - 1) / S->tx, (A.ny + S->ty - 1) / S->ty, (A.nz + A.zc - 1) / A.zc);
-            if (S->ty == 8) pe::k_stress<float, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
-            else pe::k_stress<float, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+            launch_stress<float>(S, A, S->stream);
             PE_CUDA(cudaEventRecord(ev[1], S->stream));
-            if (S->ty == 8) pe::k_velocity<float, 32, 8><<<grid, dim3(32, 8), 0, S->stream>>>(A);
-            else pe::k_velocity<float, 32, 4><<<grid, dim3(32, 4), 0, S->stream>>>(A);
+            launch_velocity<float>(S, A, S->stream);
         }
         PE_CUDA(cudaEventRecord(ev[2], S->stream));
         pe::k_step_advance<<<1, 1, 0, S->stream>>>(S->step, 1);

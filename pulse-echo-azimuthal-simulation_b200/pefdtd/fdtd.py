@@ -86,7 +86,8 @@ class DeviceSolve:
 
     def __init__(self, mats, Ct, rho_t, h, dt, coeffs, src_idx, src_w, rec_off, rec_idx, rec_w,
                  record="pressure", damped_record=False, sponge=None, damp_volume=None,
-                 dtype="float32", device=None, chunk_steps=0, tile=(0, 0), z_chunk=0):
+                 dtype="float32", device=None, chunk_steps=0, tile=(0, 0), z_chunk=0,
+                 variant="tiled"):
         torch = _torch()
         npdt, pedt = _dtype(dtype)
         self.torch = torch
@@ -116,6 +117,9 @@ class DeviceSolve:
         cfg.chunk_steps = int(chunk_steps)
         cfg.tile_x, cfg.tile_y = int(tile[0]), int(tile[1])
         cfg.z_chunk = int(z_chunk)
+        if variant not in _capi.KERNEL_VARIANT:
+            raise ValueError(f"variant must be one of {sorted(_capi.KERNEL_VARIANT)}")
+        cfg.variant = _capi.KERNEL_VARIANT[variant]
         self.cfg = cfg
         with torch.cuda.device(self.device):
             self.lab_t = torch.from_numpy(np.ascontiguousarray(mats.astype(np.uint16).view(np.int16))
@@ -240,7 +244,7 @@ def forward_fused_labels(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, ord
                          c_couplant=1500.0, rho_couplant=300.0, record="pressure", slab=32,
                          stress_smem=False, progress=None, mat_tables=None, *,
                          dtype="float32", damped_record=False, device=None, chunk_steps=0,
-                         tile=(0, 0), z_chunk=0, return_solve=False):
+                         tile=(0, 0), z_chunk=0, variant="tiled", return_solve=False):
     """Label-indexed solve; returns the (nt, n_rec) traces as float32 (float64
     when dtype="float64"). ``slab`` and ``stress_smem`` are accepted for
     signature compatibility; the kernels march z without slabs."""
@@ -289,7 +293,7 @@ def forward_fused_labels(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, ord
     solve = DeviceSolve(mats, Ct, rho_t, h, dt, coeffs, s_idx, s_w, r_off, r_idx, r_w,
                         record=record, damped_record=damped_record, sponge=sponge,
                         damp_volume=dm, dtype=dtype, device=device, chunk_steps=chunk_steps,
-                        tile=tile, z_chunk=z_chunk)
+                        tile=tile, z_chunk=z_chunk, variant=variant)
     solve.set_wavelet(np.asarray(wavelet, float)[:nt])
     try:
         _run_with_progress(solve, int(nt), progress)
@@ -353,7 +357,7 @@ def _compress_dense(C, rho, npdt):
 def forward_fused(C, rho, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coeffs=None,
                   sponge_width=0, sponge_strength=0.09, damp_mask=None, record="pressure",
                   progress=None, *, dtype="float32", device=None, chunk_steps=0, tile=(0, 0),
-                  z_chunk=0):
+                  z_chunk=0, variant="tiled"):
     """Dense-stiffness solve (C: dict of the 21 Voigt maps or scalars, rho:
     (nz, ny, nx)). Distinct media are folded into a material table and run on
     the label kernels with the dense path's end-of-step damped recording."""
@@ -369,7 +373,7 @@ def forward_fused(C, rho, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coef
     solve = DeviceSolve(mats, Ct, rho_t, h, dt, coeffs, s_idx, s_w, r_off, r_idx, r_w,
                         record=record, damped_record=True, sponge=sponge, damp_volume=dm,
                         dtype=dtype, device=device, chunk_steps=chunk_steps, tile=tile,
-                        z_chunk=z_chunk)
+                        z_chunk=z_chunk, variant=variant)
     try:
         solve.set_wavelet(np.asarray(wavelet, float)[:nt])
         _run_with_progress(solve, int(nt), progress)

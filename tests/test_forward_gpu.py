@@ -17,6 +17,22 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5   # FP32 trace rel-L2 against the reference's own update
 
 
+def _tiny(shape):
+    """A grid smaller than one stencil: random labels, probe in the middle."""
+    from pefdtd import materials
+    from pefdtd.coeffs import optimised_coeffs
+    rng = np.random.default_rng(9)
+    lab = rng.integers(-1, 3, size=shape).astype(np.int32)
+    axes = rng.normal(size=(3, 3))
+    Ct, rho = materials.material_tables(axes)
+    c = tuple(s // 2 for s in shape)
+    nt = 30
+    return dict(lab=lab, axes=axes, Ct=Ct, rho_t=rho, mats=(lab + 1).astype(np.uint16), h=1e-4,
+                dt=5e-9, nt=nt, coeffs=optimised_coeffs(8), wavelet=np.sin(np.arange(nt) * 0.3),
+                src_pts=[(c, 1.0)], rec_groups=[([c, (0, 0, 0)], np.array([0.5, 0.5]))],
+                sponge=1, record="pressure")
+
+
 def _fwd(p, **kw):
     from pefdtd import fdtd
     kw.setdefault("coeffs", p["coeffs"])
@@ -48,18 +64,24 @@ def test_bit_exact_vs_oracle_f64_and_f32_error():
     assert rel_l2(tr32, tr64) < 1e-5
 
 
-@pytest.mark.parametrize("shape,tile,zc,chunk", [
-    ((17, 23, 19), (32, 8), 0, 0),
-    ((33, 41, 37), (32, 4), 7, 13),
-    ((24, 70, 66), (32, 8), 5, 200),
-    ((40, 9, 100), (32, 4), 40, 1),
+@pytest.mark.parametrize("shape,tile,zc,chunk,variant", [
+    ((17, 23, 19), (32, 8), 0, 0, "simple"),
+    ((33, 41, 37), (32, 4), 7, 13, "simple"),
+    ((24, 70, 66), (32, 8), 5, 200, "simple"),
+    ((40, 9, 100), (32, 4), 40, 1, "simple"),
+    ((17, 23, 19), (0, 0), 0, 0, "tiled"),
+    ((33, 41, 37), (0, 0), 7, 13, "tiled"),
+    ((24, 70, 66), (0, 0), 5, 200, "tiled"),
+    ((40, 9, 100), (0, 0), 40, 1, "tiled"),
+    ((21, 97, 131), (0, 0), 0, 7, "tiled"),
+    ((3, 5, 2), (0, 0), 0, 0, "tiled"),
 ])
-def test_odd_grids_tiles_and_schedules(shape, tile, zc, chunk):
-    p = make_small(nt=60, shape=shape, n_grains=7, sponge=2)
+def test_odd_grids_tiles_and_schedules(shape, tile, zc, chunk, variant):
+    p = make_small(nt=60, shape=shape, n_grains=7, sponge=2) if min(shape) > 8 else _tiny(shape)
     from pefdtd import damping
     mask = damping.fluid_damp_mask(p["lab"], 0.05)
     tr = _fwd(p, record="pressure", damp_mask=mask, damped_record=True, tile=tile, z_chunk=zc,
-              chunk_steps=chunk)
+              chunk_steps=chunk, variant=variant)
     ref = O.run_oracle(oracle_prob(p, record="pressure", damped_record=True, damp_mask=mask),
                        fma_mode=1)
     assert np.array_equal(tr, ref)
