@@ -137,6 +137,11 @@ int pe_solver_set_wavelet(PeSolver *s, const void *wavelet, int64_t nt);
 int pe_solver_run(PeSolver *s, const PeState *state, void *traces_dev, int64_t step_begin,
                   int64_t step_end, void *stream);
 
+/* Wait for the solver's queued work and report its device status: PE_OK, or
+ * PE_ERR_TIMEOUT if a bounded device-side wait (TMA arrival) gave up, in
+ * which case the traces of the affected run are invalid. Clears the status. */
+int pe_solver_status(PeSolver *s);
+
 /* Kernel launches issued by the last pe_solver_run (diagnostics). */
 int64_t pe_solver_launch_count(const PeSolver *s);
 

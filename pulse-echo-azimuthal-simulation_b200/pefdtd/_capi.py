@@ -75,6 +75,7 @@ def lib():
         L.pe_solver_launch_count.argtypes = [C.c_void_p]
         L.pe_solver_launch_count.restype = C.c_int64
         L.pe_solver_destroy.argtypes = [C.c_void_p]
+        L.pe_solver_status.argtypes = [C.c_void_p]
         L.pe_solver_profile.argtypes = [C.c_void_p, C.POINTER(PeState), C.c_int,
                                         C.POINTER(C.c_float), C.c_void_p]
         L.pe_forward_host.argtypes = [C.POINTER(PeConfig), C.c_void_p, C.c_void_p,
@@ -108,5 +109,6 @@ def ptr(a):
 
 def exported_symbols():
     return ["pe_abi_version", "pe_last_error", "pe_solver_create", "pe_solver_set_wavelet",
-            "pe_solver_run", "pe_solver_launch_count", "pe_solver_profile", "pe_solver_destroy",
+            "pe_solver_run", "pe_solver_launch_count", "pe_solver_profile", "pe_solver_status",
+            "pe_solver_destroy",
             "pe_forward_host", "pe_label_cylinder"]

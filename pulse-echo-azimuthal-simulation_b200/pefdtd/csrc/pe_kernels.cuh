@@ -65,6 +65,7 @@ struct StepArgs {
     const long long *step;      // device: global index of chunk step 0
     int k;                      // step within the chunk
     int zc;                     // planes per z-march
+    int *status;                // device status word (bounded waits record timeouts)
 };
 
 // ---------------------------------------------------------------- helpers

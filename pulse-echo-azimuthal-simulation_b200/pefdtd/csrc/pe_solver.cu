@@ -18,6 +18,7 @@
 
 #include "pe_kernels.cuh"
 #include "pe_kernels_tiled.cuh"
+#include "pe_kernels_tma.cuh"
 #include "pefdtd.h"
 
 namespace {
@@ -89,6 +90,13 @@ struct PeSolver {
     int variant = PE_KERNEL_TILED;
     int zc_s = 0, zc_v = 0;     // planes per z-march of the stress / velocity launches
     long long launches = 0;
+    int *status = nullptr;      // device status word
+    bool tma = false;           // TMA-fed kernels in use for the current state
+    bool tma_capable = false;   // grid rows are 16-byte multiples and the driver encodes maps
+    PeState mstate{};           // state the tensor maps were encoded for
+    bool maps_ok = false;
+    pe::TmapsStress ms{};
+    pe::TmapsVelocity mv{};
 
     ~PeSolver()
     {
@@ -97,7 +105,7 @@ struct PeSolver {
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
         void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
-                        rec_pos, rec_w, grp_off, rec_val, wavelet, step};
+                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status};
         for (void *b : bufs)
             if (b) cudaFree(b);
     }
@@ -141,6 +149,7 @@ pe::StepArgs<T> make_args(const PeSolver *S, const PeState *st, int k)
     A.step = S->step;
     A.k = k;
     A.zc = S->zc_s;
+    A.status = S->status;
     return A;
 }
 
@@ -171,6 +180,11 @@ void launch_stress(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st
     A.zc = S->zc_s;
     dim3 grid((A.nx + pe::TS_OX - 1) / pe::TS_OX, (A.ny + pe::TS_OY - 1) / pe::TS_OY,
               (A.nz + A.zc - 1) / A.zc);
+    if (S->tma) {
+        pe::k_stress_tma<T><<<grid, dim3(pe::TB_X, pe::TB_Y, 1), pe::stress_tma_smem<T>(S->cfg.n_mat), st>>>(
+            S->ms, A, S->cfg.n_mat);
+        return;
+    }
     pe::k_stress_t<T><<<grid, dim3(pe::TB_X, pe::TB_Y, 1), pe::stress_tiled_smem<T>(S->cfg.n_mat), st>>>(
         A, S->cfg.n_mat);
 }
@@ -187,6 +201,11 @@ void launch_velocity(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t 
     A.zc = S->zc_v;
     dim3 grid((A.nx + pe::TB_X - 1) / pe::TB_X, (A.ny + pe::TB_Y - 1) / pe::TB_Y,
               (A.nz + A.zc - 1) / A.zc);
+    if (S->tma) {
+        pe::k_velocity_tma<T><<<grid, dim3(pe::TB_X, pe::TB_Y, 1), pe::velocity_tma_smem<T>(S->cfg.n_mat),
+                                 st>>>(S->mv, A, S->cfg.n_mat);
+        return;
+    }
     pe::k_velocity_t<T><<<grid, dim3(pe::TB_X, pe::TB_Y, 1), pe::velocity_tiled_smem<T>(S->cfg.n_mat),
                           st>>>(A, S->cfg.n_mat);
 }
@@ -261,6 +280,43 @@ int occupancy_slots(K kernel, int threads, size_t smem)
     return nsm * per;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 3-D map (x fastest) of one (nz, ny, nx) field with a (bw, bh, 1) box;
+// out-of-grid box elements read as zero
+int encode_box(CUtensorMap *m, const void *base, CUtensorMapDataType dt, int es, const PeConfig &c,
+               int bw, int bh)
+{
+    const cuuint64_t dims[3] = {(cuuint64_t)c.nx, (cuuint64_t)c.ny, (cuuint64_t)c.nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)c.nx * es, (cuuint64_t)c.nx * c.ny * es};
+    const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode_fn()(m, dt, 3, const_cast<void *>(base), dims, strides, box, estr,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PE_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return PE_OK;
+}
+
 template <typename T>
 int configure_kernels(PeSolver *S)
 {
@@ -285,10 +341,60 @@ int configure_kernels(PeSolver *S)
     PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     const long long ts = (long long)((c.nx + pe::TS_OX - 1) / pe::TS_OX) * ((c.ny + pe::TS_OY - 1) / pe::TS_OY);
     const long long tv = (long long)((c.nx + pe::TB_X - 1) / pe::TB_X) * ((c.ny + pe::TB_Y - 1) / pe::TB_Y);
-    const int ss = occupancy_slots(pe::k_stress_t<T>, pe::TB_X * pe::TB_Y, need_s);
-    const int sv = occupancy_slots(pe::k_velocity_t<T>, pe::TB_X * pe::TB_Y, need_v);
+    int ss = occupancy_slots(pe::k_stress_t<T>, pe::TB_X * pe::TB_Y, need_s);
+    int sv = occupancy_slots(pe::k_velocity_t<T>, pe::TB_X * pe::TB_Y, need_v);
+    // TMA path: rows must be whole 16-byte units (box x-origins are multiples of 4 elements)
+    const size_t tms = pe::stress_tma_smem<T>(c.n_mat), tmv = pe::velocity_tma_smem<T>(c.n_mat);
+    S->tma_capable = c.nx % 4 == 0 && tms <= (size_t)optin && tmv <= (size_t)optin &&
+                     encode_fn() != nullptr;
+    if (S->tma_capable) {
+        PE_CUDA(cudaFuncSetAttribute(pe::k_stress_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        ss = occupancy_slots(pe::k_stress_tma<T>, pe::TB_X * pe::TB_Y, tms);
+        sv = occupancy_slots(pe::k_velocity_tma<T>, pe::TB_X * pe::TB_Y, tmv);
+    }
     S->zc_s = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, ts, ss, 4);
     S->zc_v = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tv, sv, 3);
+    return PE_OK;
+}
+
+// Tensor maps of the nine fields (and the damping volume) for the TMA
+// kernels; re-encoded whenever the caller's state buffers change. Falls back
+// to the cp.async kernels when a buffer is not 16-byte aligned.
+int ensure_maps(PeSolver *S, const PeState *st)
+{
+    if (!S->tma_capable) {
+        S->tma = false;
+        return PE_OK;
+    }
+    if (S->maps_ok && same_state(S->mstate, *st)) return PE_OK;
+    const PeConfig &c = S->cfg;
+    const int es = S->esize;
+    bool aligned = !S->dvol || ((uintptr_t)S->dvol % 16) == 0;
+    for (int i = 0; i < 3; ++i) aligned = aligned && ((uintptr_t)st->v[i] % 16) == 0;
+    for (int i = 0; i < 6; ++i) aligned = aligned && ((uintptr_t)st->s[i] % 16) == 0;
+    S->mstate = *st;
+    S->maps_ok = true;
+    S->tma = aligned;
+    if (!aligned) return PE_OK;
+    const CUtensorMapDataType dt = es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    int rc;
+    for (int f = 0; f < 3; ++f)
+        if ((rc = encode_box(&S->ms.vt[f], st->v[f], dt, es, c, pe::KS_VW, pe::KS_VH))) return rc;
+    for (int f = 0; f < 6; ++f)
+        if ((rc = encode_box(&S->ms.sc[f], st->s[f], dt, es, c, pe::KS_SW, pe::KS_SH))) return rc;
+    const int vf[5] = {0, 1, 3, 4, 5};
+    for (int f = 0; f < 5; ++f)
+        if ((rc = encode_box(&S->mv.st[f], st->s[vf[f]], dt, es, c, pe::KV_SW, pe::KV_SH))) return rc;
+    for (int f = 0; f < 3; ++f)
+        if ((rc = encode_box(&S->mv.vc[f], st->v[f], dt, es, c, pe::KV_CW, pe::KV_CH))) return rc;
+    if (S->dvol) {
+        if ((rc = encode_box(&S->ms.dv, S->dvol, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c, pe::KS_SW, pe::KS_SH))) return rc;
+        if ((rc = encode_box(&S->mv.dv, S->dvol, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c, pe::KV_CW, pe::KV_CH))) return rc;
+    } else {
+        std::memset(&S->ms.dv, 0, sizeof(S->ms.dv));
+        std::memset(&S->mv.dv, 0, sizeof(S->mv.dv));
+    }
     return PE_OK;
 }
 
@@ -406,6 +512,8 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     if ((rc = dev_alloc(&S->c21, (size_t)es * pe::C21_STRIDE * c.n_mat))) return rc;
     if ((rc = dev_alloc(&S->rho, (size_t)es * c.n_mat))) return rc;
     if ((rc = dev_alloc(&S->step, sizeof(long long)))) return rc;
+    if ((rc = dev_alloc(&S->status, sizeof(int)))) return rc;
+    PE_CUDA(cudaMemsetAsync(S->status, 0, sizeof(int), st));
 
     // labels: copy + range check, then mark source / receiver cells
     unsigned long long *nbad = nullptr;
@@ -504,6 +612,10 @@ int pe_solver_run(PeSolver *S, const PeState *state, void *traces, int64_t b, in
     for (int i = 0; i < 6; ++i)
         if (!state->s[i]) return fail(PE_ERR_INVALID, "state field missing");
     S->launches = 0;
+    {
+        const int rc0 = ensure_maps(S, state);
+        if (rc0) return rc0;
+    }
     if (e == b) return PE_OK;
     cudaStream_t user = (cudaStream_t)stream;
     PE_CUDA(cudaEventRecord(S->ev_in, user));
@@ -549,6 +661,20 @@ int pe_solver_run(PeSolver *S, const PeState *state, void *traces, int64_t b, in
 
 int64_t pe_solver_launch_count(const PeSolver *S) { return S ? S->launches : -1; }
 
+int pe_solver_status(PeSolver *S)
+{
+    if (!S) return fail(PE_ERR_INVALID, "null solver");
+    int st = 0;
+    PE_CUDA(cudaStreamSynchronize(S->stream));
+    PE_CUDA(cudaMemcpy(&st, S->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+        PE_CUDA(cudaMemset(S->status, 0, sizeof(int)));
+        return fail(st == PE_ERR_TIMEOUT ? PE_ERR_TIMEOUT : PE_ERR_CUDA,
+                    "a bounded device-side wait gave up; the results of the affected steps are invalid");
+    }
+    return PE_OK;
+}
+
 int pe_solver_profile(PeSolver *S, const PeState *state, int n_steps, float *ms_out, void *stream)
 {
     if (!S || !state || !ms_out || n_steps < 1) return fail(PE_ERR_INVALID, "bad profile request");
@@ -558,6 +684,10 @@ int pe_solver_profile(PeSolver *S, const PeState *state, int n_steps, float *ms_
     for (auto &e : ev) PE_CUDA(cudaEventCreate(&e));
     PE_CUDA(cudaEventRecord(S->ev_in, user));
     PE_CUDA(cudaStreamWaitEvent(S->stream, S->ev_in, 0));
+    {
+        const int rc0 = ensure_maps(S, state);
+        if (rc0) return rc0;
+    }
     pe::k_step_set<<<1, 1, 0, S->stream>>>(S->step, 0);
     float tot_s = 0.f, tot_v = 0.f;
     const int saved_chunk = S->chunk;

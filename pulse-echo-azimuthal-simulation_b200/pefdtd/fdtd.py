@@ -211,8 +211,13 @@ class DeviceSolve:
         except Exception:
             pass
 
+    def check_status(self):
+        """Raise if a bounded device-side wait of the queued work gave up."""
+        _capi.check(self._L.pe_solver_status(self._h))
+
     def traces_numpy(self, nt=None):
         nt = self.nt if nt is None else nt
+        self.check_status()
         return self.traces[:nt, :self.n_groups].cpu().numpy()
 
 

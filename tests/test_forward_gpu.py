@@ -51,8 +51,9 @@ def test_bit_exact_vs_oracle_f32(record, damped):
     assert np.array_equal(tr, ref), f"max |diff| {np.abs(tr - ref).max()}"
 
 
-def test_bit_exact_vs_oracle_f64_and_f32_error():
-    p = make_small(nt=150, shape=(22, 26, 30), n_grains=10, sponge=4)
+@pytest.mark.parametrize("shape", [(22, 26, 30), (21, 37, 72)])
+def test_bit_exact_vs_oracle_f64_and_f32_error(shape):
+    p = make_small(nt=150, shape=shape, n_grains=10, sponge=4)
     from pefdtd.fdtd import _material_tables64
     Ct, rho = _material_tables64(p["axes"], 1500.0, 300.0)
     tr64 = _fwd(p, record="pressure", damped_record=True, dtype="float64")
@@ -75,6 +76,10 @@ def test_bit_exact_vs_oracle_f64_and_f32_error():
     ((40, 9, 100), (0, 0), 40, 1, "tiled"),
     ((21, 97, 131), (0, 0), 0, 7, "tiled"),
     ((3, 5, 2), (0, 0), 0, 0, "tiled"),
+    # nx % 4 == 0: the TMA-fed kernels (box loads, mbarrier slots)
+    ((23, 45, 68), (0, 0), 0, 11, "tiled"),
+    ((19, 71, 132), (0, 0), 6, 200, "tiled"),
+    ((9, 8, 4), (0, 0), 0, 0, "tiled"),
 ])
 def test_odd_grids_tiles_and_schedules(shape, tile, zc, chunk, variant):
     p = make_small(nt=60, shape=shape, n_grains=7, sponge=2) if min(shape) > 8 else _tiny(shape)
