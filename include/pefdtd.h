@@ -166,6 +166,31 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host,
                     const PeProbe *probe, const void *wavelet_host, int64_t nt,
                     void *traces_host);
 
+/* ---- Batches: many independent solves advanced together ----------------
+ * No counterpart in the reference, which runs one azimuth at a time in a
+ * Python loop (sim/pipeline/sweep_runner.py:322-390); the closest precedent
+ * is ringfwi's elastic3d.forward_batch (vendor/ringfwi/elastic3d.py:474-632),
+ * which stacks transmits on a leading array axis. Every solve keeps the
+ * single-solve contract above (own grid size, medium, probe, wavelet, state
+ * and traces); all share one dtype, the tiled kernels, nx a multiple of 4 and
+ * 16-byte aligned state buffers. Each step is one stress and one velocity
+ * launch covering every solve; chunks of steps replay as CUDA graphs. */
+typedef struct PeBatch PeBatch;
+
+int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const PeProbe *probes,
+                    PeBatch **out);
+/* Work layout: planes per z-march (0 = 40) and steps per captured graph
+ * (0 = keep). Chosen by pefdtd.autotune. */
+int pe_batch_schedule(PeBatch *b, int z_chunk, int chunk_steps);
+int pe_batch_set_wavelet(PeBatch *b, int i, const void *wavelet, int64_t nt);
+/* Advance every solve i over [step_begin, step_end): states[i], traces[i] as
+ * in pe_solver_run. Asynchronous on `stream`. */
+int pe_batch_run(PeBatch *b, const PeState *states, void *const *traces, int64_t step_begin,
+                 int64_t step_end, void *stream);
+int pe_batch_status(PeBatch *b);
+int64_t pe_batch_launch_count(const PeBatch *b);
+int pe_batch_destroy(PeBatch *b);
+
 /* Power-diagram labels of a cylinder (specimen builder, reference
  * sim/core/specimen.py:298-337): out_dev[(iz*ny + iy)*nx + ix] = the seed
  * minimising ((x-sx)^2 + (y-sy)^2) - w + (z-sz)^2 in float64 at point

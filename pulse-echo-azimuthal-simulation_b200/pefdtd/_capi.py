@@ -81,6 +81,16 @@ def lib():
         L.pe_forward_host.argtypes = [C.POINTER(PeConfig), C.c_void_p, C.c_void_p,
                                       C.POINTER(PeMedium), C.POINTER(PeProbe), C.c_void_p,
                                       C.c_int64, C.c_void_p]
+        L.pe_batch_create.argtypes = [C.c_int, C.POINTER(PeConfig), C.POINTER(PeMedium),
+                                      C.POINTER(PeProbe), C.POINTER(C.c_void_p)]
+        L.pe_batch_schedule.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.pe_batch_set_wavelet.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+        L.pe_batch_run.argtypes = [C.c_void_p, C.POINTER(PeState), C.POINTER(C.c_void_p),
+                                   C.c_int64, C.c_int64, C.c_void_p]
+        L.pe_batch_status.argtypes = [C.c_void_p]
+        L.pe_batch_launch_count.argtypes = [C.c_void_p]
+        L.pe_batch_launch_count.restype = C.c_int64
+        L.pe_batch_destroy.argtypes = [C.c_void_p]
         L.pe_label_cylinder.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                         C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_void_p]
@@ -111,4 +121,6 @@ def exported_symbols():
     return ["pe_abi_version", "pe_last_error", "pe_solver_create", "pe_solver_set_wavelet",
             "pe_solver_run", "pe_solver_launch_count", "pe_solver_profile", "pe_solver_status",
             "pe_solver_destroy",
-            "pe_forward_host", "pe_label_cylinder"]
+            "pe_forward_host", "pe_label_cylinder", "pe_batch_create", "pe_batch_schedule",
+            "pe_batch_set_wavelet", "pe_batch_run", "pe_batch_status", "pe_batch_launch_count",
+            "pe_batch_destroy"]

@@ -151,17 +151,18 @@ __device__ __forceinline__ void strain_column(const StepArgs<T> &A, int q, const
 template <typename T, int NC, bool EDGE>
 __device__ __forceinline__ void stress_tma_run(const TmapsStress &M, const StepArgs<T> &A, T *vslots,
                                                T *sslots, T *gs, unsigned long long *bars,
-                                               const T *tab, bool tab_smem, bool has_dvol)
+                                               const T *tab, bool tab_smem, bool has_dvol,
+                                               int bx, int by, int bz)
 {
     constexpr int PV = pad128<T>(KS_VSZ), PS = pad128<T>(KS_SSZ);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TB_X + tx;
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const long long sy = A.sy, sz = A.sz;
-    const int X0 = blockIdx.x * TS_OX - 1, Y0 = blockIdx.y * TS_OY - 1;
+    const int X0 = bx * TS_OX - 1, Y0 = by * TS_OY - 1;
     const int gx = X0 + tx, gy = Y0 + ty;
     const bool col_ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
     const int col = col_ok ? (int)(gy * sy + gx) : 0;
-    const int zb = blockIdx.z * A.zc;
+    const int zb = bz * A.zc;
     const int ze = min(zb + A.zc, nz);
     const long long n = *A.step + A.k;
     const T wn = A.n_src ? A.wavelet[n] : T(0);
@@ -317,13 +318,16 @@ __device__ __forceinline__ void stress_tma_run(const TmapsStress &M, const StepA
     }
 }
 
+// One block's share of a stress launch: tile (bx, by), z-chunk bz. The
+// material table is (re)loaded into shared memory when load_table is set; the
+// caller guarantees the block is between barriers (no copy in flight).
 template <typename T>
-__global__ void __launch_bounds__(TB_N, 1) k_stress_tma(const __grid_constant__ TmapsStress M,
-                                                        const StepArgs<T> A, int n_mat)
+__device__ __forceinline__ void stress_tma_block(const TmapsStress &M, const StepArgs<T> &A, int n_mat,
+                                                 unsigned char *smem, int bx, int by, int bz,
+                                                 bool load_table)
 {
-    extern __shared__ __align__(128) unsigned char smem_tma[];
-    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_tma);
-    T *vslots = reinterpret_cast<T *>(smem_tma + 128);
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem);
+    T *vslots = reinterpret_cast<T *>(smem + 128);
     T *sslots = vslots + 3 * (size_t)ks_slot_v<T>();
     T *gs = sslots + 3 * (size_t)ks_slot_s<T>();
     T *tsm = gs + (size_t)3 * 6 * TB_N;
@@ -333,20 +337,28 @@ __global__ void __launch_bounds__(TB_N, 1) k_stress_tma(const __grid_constant__ 
         fence_mbar_init();
     }
     const bool tab_smem = table_in_smem<T>(n_mat);
-    if (tab_smem)
+    if (tab_smem && load_table)
         for (int i = tid; i < n_mat * C21_STRIDE; i += TB_N) tsm[i] = A.c21[i];
     __syncthreads();
     const T *tab = tab_smem ? tsm : A.c21;
     const bool has_dvol = A.dvol != nullptr;
-    const int X0 = blockIdx.x * TS_OX - 1, Y0 = blockIdx.y * TS_OY - 1;
+    const int X0 = bx * TS_OX - 1, Y0 = by * TS_OY - 1;
     const bool inner = X0 - T_H >= 0 && X0 + TB_X - 1 + T_H < A.nx && Y0 - T_H >= 0 &&
                        Y0 + TB_Y - 1 + T_H < A.ny;
     if (A.nc == 4) {
-        if (inner) stress_tma_run<T, 4, false>(M, A, vslots, sslots, gs, bars, tab, tab_smem, has_dvol);
-        else stress_tma_run<T, 4, true>(M, A, vslots, sslots, gs, bars, tab, tab_smem, has_dvol);
+        if (inner) stress_tma_run<T, 4, false>(M, A, vslots, sslots, gs, bars, tab, tab_smem, has_dvol, bx, by, bz);
+        else stress_tma_run<T, 4, true>(M, A, vslots, sslots, gs, bars, tab, tab_smem, has_dvol, bx, by, bz);
     } else {
-        stress_tma_run<T, 0, true>(M, A, vslots, sslots, gs, bars, tab, tab_smem, has_dvol);
+        stress_tma_run<T, 0, true>(M, A, vslots, sslots, gs, bars, tab, tab_smem, has_dvol, bx, by, bz);
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TB_N, 1) k_stress_tma(const __grid_constant__ TmapsStress M,
+                                                        const StepArgs<T> A, int n_mat)
+{
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    stress_tma_block<T>(M, A, n_mat, smem_tma, blockIdx.x, blockIdx.y, blockIdx.z, true);
 }
 
 // ---------------------------------------------------------------- velocity
@@ -386,17 +398,17 @@ __device__ __forceinline__ void vel_taps(const StepArgs<T> &A, int z, const T *t
 template <typename T, int NC, bool EDGE>
 __device__ __forceinline__ void velocity_tma_run(const TmapsVelocity &M, const StepArgs<T> &A, T *slots,
                                                  unsigned long long *bars, const T *rho_tab,
-                                                 bool has_dvol)
+                                                 bool has_dvol, int bx, int by, int bz)
 {
     constexpr int PT = pad128<T>(KV_SSZ), PC = pad128<T>(KV_CSZ), SL = kv_slot<T>();
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TB_X + tx;
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const long long sy = A.sy, sz = A.sz;
-    const int x0 = blockIdx.x * TB_X, y0 = blockIdx.y * TB_Y;
+    const int x0 = bx * TB_X, y0 = by * TB_Y;
     const int ix = x0 + tx, iy = y0 + ty;
     const bool out_ok = ix < nx && iy < ny;
     const int col = out_ok ? (int)(iy * sy + ix) : 0;
-    const int zb = blockIdx.z * A.zc;
+    const int zb = bz * A.zc;
     const int ze = min(zb + A.zc, nz);
     const bool leader = tid == 0;
     const unsigned bytes = 5u * KV_SSZ * sizeof(T) + 3u * KV_CSZ * sizeof(T) + (has_dvol ? KV_CSZ * 4u : 0u);
@@ -512,12 +524,12 @@ __device__ __forceinline__ void velocity_tma_run(const TmapsVelocity &M, const S
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TB_N, 1) k_velocity_tma(const __grid_constant__ TmapsVelocity M,
-                                                          const StepArgs<T> A, int n_mat)
+__device__ __forceinline__ void velocity_tma_block(const TmapsVelocity &M, const StepArgs<T> &A, int n_mat,
+                                                   unsigned char *smem, int bx, int by, int bz,
+                                                   bool load_table)
 {
-    extern __shared__ __align__(128) unsigned char smem_tma[];
-    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_tma);
-    T *slots = reinterpret_cast<T *>(smem_tma + 128);
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem);
+    T *slots = reinterpret_cast<T *>(smem + 128);
     T *rsm = slots + 3 * (size_t)kv_slot<T>();
     const int tid = threadIdx.y * TB_X + threadIdx.x;
     if (tid == 0) {
@@ -525,19 +537,91 @@ __global__ void __launch_bounds__(TB_N, 1) k_velocity_tma(const __grid_constant_
         fence_mbar_init();
     }
     const bool tab_smem = table_in_smem<T>(n_mat);
-    if (tab_smem)
+    if (tab_smem && load_table)
         for (int i = tid; i < n_mat; i += TB_N) rsm[i] = A.rho[i];
     __syncthreads();
     const T *rho_tab = tab_smem ? rsm : A.rho;
     const bool has_dvol = A.dvol != nullptr;
-    const int x0 = blockIdx.x * TB_X, y0 = blockIdx.y * TB_Y;
+    const int x0 = bx * TB_X, y0 = by * TB_Y;
     const bool inner = x0 - T_H >= 0 && x0 + TB_X - 1 + T_H < A.nx && y0 - T_H >= 0 &&
                        y0 + TB_Y - 1 + T_H < A.ny;
     if (A.nc == 4) {
-        if (inner) velocity_tma_run<T, 4, false>(M, A, slots, bars, rho_tab, has_dvol);
-        else velocity_tma_run<T, 4, true>(M, A, slots, bars, rho_tab, has_dvol);
+        if (inner) velocity_tma_run<T, 4, false>(M, A, slots, bars, rho_tab, has_dvol, bx, by, bz);
+        else velocity_tma_run<T, 4, true>(M, A, slots, bars, rho_tab, has_dvol, bx, by, bz);
     } else {
-        velocity_tma_run<T, 0, true>(M, A, slots, bars, rho_tab, has_dvol);
+        velocity_tma_run<T, 0, true>(M, A, slots, bars, rho_tab, has_dvol, bx, by, bz);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TB_N, 1) k_velocity_tma(const __grid_constant__ TmapsVelocity M,
+                                                          const StepArgs<T> A, int n_mat)
+{
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    velocity_tma_block<T>(M, A, n_mat, smem_tma, blockIdx.x, blockIdx.y, blockIdx.z, true);
+}
+
+// ---------------------------------------------------------------- batches
+// A batch of solves of any grid sizes advances one step per launch pair. Work
+// items (solve, tile x, tile y, z-chunk) are listed solve by solve; each
+// resident block walks a contiguous run of items, re-staging the solve's
+// arguments and material table only when the solve changes.
+struct BatchItem {
+    int solve, bx, by, bz;
+};
+
+template <typename T>
+__device__ __forceinline__ void copy_args(StepArgs<T> *dst, const StepArgs<T> *src, int k)
+{
+    const int tid = threadIdx.y * TB_X + threadIdx.x;
+    const int nw = (int)(sizeof(StepArgs<T>) / 4);
+    for (int i = tid; i < nw; i += TB_N)
+        reinterpret_cast<int *>(dst)[i] = reinterpret_cast<const int *>(src)[i];
+    __syncthreads();
+    if (tid == 0) dst->k = k;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TB_N, 1)
+    k_stress_tma_batch(const StepArgs<T> *__restrict__ descs, const TmapsStress *__restrict__ maps,
+                       const int *__restrict__ n_mats, const BatchItem *__restrict__ items, int n_items,
+                       int k)
+{
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    __shared__ __align__(16) StepArgs<T> As;
+    const int per = (n_items + gridDim.x - 1) / gridDim.x;
+    const int i0 = blockIdx.x * per, i1 = min(n_items, i0 + per);
+    int cur = -1;
+    for (int it = i0; it < i1; ++it) {
+        const BatchItem w = items[it];
+        __syncthreads();   // the previous item is finished by every thread
+        const bool fresh = w.solve != cur;
+        if (fresh) copy_args(&As, descs + w.solve, k);
+        __syncthreads();
+        stress_tma_block<T>(maps[w.solve], As, n_mats[w.solve], smem_tma, w.bx, w.by, w.bz, fresh);
+        cur = w.solve;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TB_N, 1)
+    k_velocity_tma_batch(const StepArgs<T> *__restrict__ descs, const TmapsVelocity *__restrict__ maps,
+                         const int *__restrict__ n_mats, const BatchItem *__restrict__ items, int n_items,
+                         int k)
+{
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    __shared__ __align__(16) StepArgs<T> As;
+    const int per = (n_items + gridDim.x - 1) / gridDim.x;
+    const int i0 = blockIdx.x * per, i1 = min(n_items, i0 + per);
+    int cur = -1;
+    for (int it = i0; it < i1; ++it) {
+        const BatchItem w = items[it];
+        __syncthreads();
+        const bool fresh = w.solve != cur;
+        if (fresh) copy_args(&As, descs + w.solve, k);
+        __syncthreads();
+        velocity_tma_block<T>(maps[w.solve], As, n_mats[w.solve], smem_tma, w.bx, w.by, w.bz, fresh);
+        cur = w.solve;
     }
 }
 

@@ -791,3 +791,306 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host, const floa
 }
 
 }  // extern "C"
+
+// ===================================================================== batches
+// A batch advances many independent solves (any grid sizes, one dtype) with
+// one stress and one velocity launch per step for all of them, replayed as
+// captured CUDA graphs of `chunk` steps. Each solve keeps its own solver-owned
+// buffers (a PeSolver); the batch owns the shared step counter and status
+// word, the per-solve argument blocks and tensor maps in device memory, and
+// the work-item lists.
+struct PeBatch {
+    std::vector<PeSolver *> solves;
+    int dtype = PE_F32, esize = 4;
+    long long *step = nullptr;
+    int *status = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    void *descs = nullptr;
+    pe::TmapsStress *maps_s = nullptr;
+    pe::TmapsVelocity *maps_v = nullptr;
+    int *nmats = nullptr;
+    pe::BatchItem *items_s = nullptr, *items_v = nullptr;
+    int n_items_s = 0, n_items_v = 0;
+    int grid_s = 1, grid_v = 1;
+    size_t smem_s = 0, smem_v = 0;
+    int z_chunk = 0, chunk = 200;
+    std::vector<PeState> states;
+    std::vector<void *> traces;
+    bool uploaded = false;
+    cudaGraphExec_t gexec = nullptr;
+    long long launches = 0;
+
+    ~PeBatch()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (stream) cudaStreamSynchronize(stream);
+        for (PeSolver *s : solves) pe_solver_destroy(s);
+        void *bufs[] = {step, status, descs, maps_s, maps_v, nmats, items_s, items_v};
+        for (void *b : bufs)
+            if (b) cudaFree(b);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <typename T>
+int batch_layout(PeBatch *B)
+{
+    std::vector<pe::BatchItem> is, iv;
+    int max_mat = 1;
+    for (int s = 0; s < (int)B->solves.size(); ++s) {
+        const PeConfig &c = B->solves[s]->cfg;
+        max_mat = std::max(max_mat, c.n_mat);
+        const int target = c.z_chunk > 0 ? c.z_chunk : (B->z_chunk > 0 ? B->z_chunk : 40);
+        const int nch = std::max(1, (c.nz + target - 1) / target);
+        const int zc = (c.nz + nch - 1) / nch;
+        B->solves[s]->zc_s = zc;
+        B->solves[s]->zc_v = zc;
+        const int nzc = (c.nz + zc - 1) / zc;
+        for (int bz = 0; bz < nzc; ++bz) {
+            for (int by = 0; by < (c.ny + pe::TS_OY - 1) / pe::TS_OY; ++by)
+                for (int bx = 0; bx < (c.nx + pe::TS_OX - 1) / pe::TS_OX; ++bx) is.push_back({s, bx, by, bz});
+            for (int by = 0; by < (c.ny + pe::TB_Y - 1) / pe::TB_Y; ++by)
+                for (int bx = 0; bx < (c.nx + pe::TB_X - 1) / pe::TB_X; ++bx) iv.push_back({s, bx, by, bz});
+        }
+    }
+    int dev = 0, optin = 0, nsm = 148;
+    PE_CUDA(cudaGetDevice(&dev));
+    PE_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    PE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    B->smem_s = pe::stress_tma_smem<T>(max_mat);
+    B->smem_v = pe::velocity_tma_smem<T>(max_mat);
+    cudaFuncAttributes fa_s{}, fa_v{};
+    PE_CUDA(cudaFuncGetAttributes(&fa_s, pe::k_stress_tma_batch<T>));
+    PE_CUDA(cudaFuncGetAttributes(&fa_v, pe::k_velocity_tma_batch<T>));
+    const int dyn_s = optin - (int)fa_s.sharedSizeBytes, dyn_v = optin - (int)fa_v.sharedSizeBytes;
+    if (B->smem_s > (size_t)dyn_s || B->smem_v > (size_t)dyn_v)
+        return fail(PE_ERR_UNSUPPORTED, "material table too large for the batched kernels");
+    PE_CUDA(cudaFuncSetAttribute(pe::k_stress_tma_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_s));
+    PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_tma_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_v));
+    int per_s = 1, per_v = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, pe::k_stress_tma_batch<T>, pe::TB_N, B->smem_s);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_v, pe::k_velocity_tma_batch<T>, pe::TB_N, B->smem_v);
+    B->n_items_s = (int)is.size();
+    B->n_items_v = (int)iv.size();
+    B->grid_s = std::max(1, std::min(B->n_items_s, nsm * std::max(1, per_s)));
+    B->grid_v = std::max(1, std::min(B->n_items_v, nsm * std::max(1, per_v)));
+    if (B->items_s) cudaFree(B->items_s);
+    if (B->items_v) cudaFree(B->items_v);
+    B->items_s = B->items_v = nullptr;
+    int rc;
+    if ((rc = dev_alloc(&B->items_s, sizeof(pe::BatchItem) * is.size()))) return rc;
+    if ((rc = dev_alloc(&B->items_v, sizeof(pe::BatchItem) * iv.size()))) return rc;
+    PE_CUDA(cudaMemcpy(B->items_s, is.data(), sizeof(pe::BatchItem) * is.size(), cudaMemcpyHostToDevice));
+    PE_CUDA(cudaMemcpy(B->items_v, iv.data(), sizeof(pe::BatchItem) * iv.size(), cudaMemcpyHostToDevice));
+    if (B->gexec) {
+        cudaGraphExecDestroy(B->gexec);
+        B->gexec = nullptr;
+    }
+    return PE_OK;
+}
+
+template <typename T>
+int batch_upload(PeBatch *B, const PeState *states, void *const *traces)
+{
+    const int n = (int)B->solves.size();
+    bool same = B->uploaded && (int)B->states.size() == n;
+    for (int s = 0; same && s < n; ++s) same = same_state(B->states[s], states[s]) && B->traces[s] == traces[s];
+    if (same) return PE_OK;
+    std::vector<pe::StepArgs<T>> descs(n);
+    std::vector<pe::TmapsStress> ms(n);
+    std::vector<pe::TmapsVelocity> mv(n);
+    for (int s = 0; s < n; ++s) {
+        PeSolver *S = B->solves[s];
+        int rc = ensure_maps(S, &states[s]);
+        if (rc) return rc;
+        if (!S->tma) return fail(PE_ERR_UNSUPPORTED, "batched solves need 16-byte aligned state buffers");
+        descs[s] = make_args<T>(S, &states[s], 0);
+        descs[s].step = B->step;
+        descs[s].status = B->status;
+        descs[s].zc = S->zc_s;
+        ms[s] = S->ms;
+        mv[s] = S->mv;
+    }
+    PE_CUDA(cudaMemcpy(B->descs, descs.data(), sizeof(pe::StepArgs<T>) * n, cudaMemcpyHostToDevice));
+    PE_CUDA(cudaMemcpy(B->maps_s, ms.data(), sizeof(pe::TmapsStress) * n, cudaMemcpyHostToDevice));
+    PE_CUDA(cudaMemcpy(B->maps_v, mv.data(), sizeof(pe::TmapsVelocity) * n, cudaMemcpyHostToDevice));
+    B->states.assign(states, states + n);
+    B->traces.assign(traces, traces + n);
+    B->uploaded = true;
+    if (B->gexec) {
+        cudaGraphExecDestroy(B->gexec);
+        B->gexec = nullptr;
+    }
+    return PE_OK;
+}
+
+template <typename T>
+int batch_chunk(PeBatch *B, int len)
+{
+    const dim3 block(pe::TB_X, pe::TB_Y, 1);
+    for (int k = 0; k < len; ++k) {
+        pe::k_stress_tma_batch<T><<<B->grid_s, block, B->smem_s, B->stream>>>(
+            (const pe::StepArgs<T> *)B->descs, B->maps_s, B->nmats, B->items_s, B->n_items_s, k);
+        pe::k_velocity_tma_batch<T><<<B->grid_v, block, B->smem_v, B->stream>>>(
+            (const pe::StepArgs<T> *)B->descs, B->maps_v, B->nmats, B->items_v, B->n_items_v, k);
+        B->launches += 2;
+    }
+    for (int s = 0; s < (int)B->solves.size(); ++s) {
+        PeSolver *S = B->solves[s];
+        if (S->n_groups <= 0) continue;
+        const int nthr = len * S->n_groups;
+        pe::k_reduce_traces<T><<<(nthr + 127) / 128, 128, 0, B->stream>>>(
+            (const T *)S->rec_val, (const T *)S->rec_w, S->grp_off, S->n_groups, S->n_rec, len, B->step,
+            (T *)B->traces[s]);
+        B->launches += 1;
+    }
+    pe::k_step_advance<<<1, 1, 0, B->stream>>>(B->step, len);
+    B->launches += 1;
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+template <typename T>
+int batch_run_t(PeBatch *B, const PeState *states, void *const *traces, int64_t b, int64_t e, cudaStream_t user)
+{
+    int rc = batch_upload<T>(B, states, traces);
+    if (rc) return rc;
+    PE_CUDA(cudaEventRecord(B->ev_in, user));
+    PE_CUDA(cudaStreamWaitEvent(B->stream, B->ev_in, 0));
+    pe::k_step_set<<<1, 1, 0, B->stream>>>(B->step, b);
+    B->launches += 1;
+    for (int64_t n = b; n < e;) {
+        const int len = (int)std::min<int64_t>(B->chunk, e - n);
+        if (len == B->chunk) {
+            if (!B->gexec) {
+                cudaGraph_t g = nullptr;
+                PE_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+                const long long before = B->launches;
+                rc = batch_chunk<T>(B, len);
+                cudaError_t ce = cudaStreamEndCapture(B->stream, &g);
+                if (rc) return rc;
+                if (ce != cudaSuccess) return fail(PE_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+                B->launches = before;
+                ce = cudaGraphInstantiate(&B->gexec, g, 0);
+                cudaGraphDestroy(g);
+                if (ce != cudaSuccess) return fail(PE_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ce));
+            }
+            PE_CUDA(cudaGraphLaunch(B->gexec, B->stream));
+            int nred = 0;
+            for (PeSolver *S : B->solves) nred += S->n_groups > 0;
+            B->launches += 2LL * len + nred + 1;
+        } else if ((rc = batch_chunk<T>(B, len))) {
+            return rc;
+        }
+        n += len;
+    }
+    PE_CUDA(cudaEventRecord(B->ev_out, B->stream));
+    PE_CUDA(cudaStreamWaitEvent(user, B->ev_out, 0));
+    return PE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const PeProbe *probes,
+                    PeBatch **out)
+{
+    if (n < 1 || !cfgs || !media || !probes || !out) return fail(PE_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    std::unique_ptr<PeBatch> B(new PeBatch());
+    B->dtype = cfgs[0].dtype;
+    B->esize = dtype_size(B->dtype);
+    for (int s = 0; s < n; ++s) {
+        if (cfgs[s].dtype != B->dtype) return fail(PE_ERR_INVALID, "all solves of a batch share one dtype");
+        if (cfgs[s].variant != PE_KERNEL_TILED)
+            return fail(PE_ERR_UNSUPPORTED, "batches run the tiled kernels");
+        PeSolver *S = nullptr;
+        int rc = pe_solver_create(&cfgs[s], &media[s], &probes[s], &S);
+        if (rc) return fail(rc, "solve " + std::to_string(s) + ": " + g_err);
+        B->solves.push_back(S);
+        if (!S->tma_capable)
+            return fail(PE_ERR_UNSUPPORTED, "solve " + std::to_string(s) +
+                                                ": batched solves need nx a multiple of 4");
+        B->chunk = std::max(B->chunk, 1);
+    }
+    B->chunk = cfgs[0].chunk_steps > 0 ? cfgs[0].chunk_steps : 200;
+    int rc;
+    if ((rc = dev_alloc(&B->step, sizeof(long long)))) return rc;
+    if ((rc = dev_alloc(&B->status, sizeof(int)))) return rc;
+    PE_CUDA(cudaMemset(B->status, 0, sizeof(int)));
+    const size_t ds = B->dtype == PE_F64 ? sizeof(pe::StepArgs<double>) : sizeof(pe::StepArgs<float>);
+    if ((rc = dev_alloc(&B->descs, ds * n))) return rc;
+    if ((rc = dev_alloc(&B->maps_s, sizeof(pe::TmapsStress) * n))) return rc;
+    if ((rc = dev_alloc(&B->maps_v, sizeof(pe::TmapsVelocity) * n))) return rc;
+    if ((rc = dev_alloc(&B->nmats, sizeof(int) * n))) return rc;
+    std::vector<int> nm(n);
+    for (int s = 0; s < n; ++s) nm[s] = cfgs[s].n_mat;
+    PE_CUDA(cudaMemcpy(B->nmats, nm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    PE_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    PE_CUDA(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming));
+    PE_CUDA(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming));
+    rc = B->dtype == PE_F64 ? batch_layout<double>(B.get()) : batch_layout<float>(B.get());
+    if (rc) return rc;
+    *out = B.release();
+    return PE_OK;
+}
+
+int pe_batch_schedule(PeBatch *B, int z_chunk, int chunk_steps)
+{
+    if (!B || z_chunk < 0 || chunk_steps < 0) return fail(PE_ERR_INVALID, "bad schedule");
+    B->z_chunk = z_chunk;
+    if (chunk_steps > 0) B->chunk = chunk_steps;
+    for (PeSolver *S : B->solves) S->cfg.z_chunk = 0;
+    B->uploaded = false;
+    return B->dtype == PE_F64 ? batch_layout<double>(B) : batch_layout<float>(B);
+}
+
+int pe_batch_set_wavelet(PeBatch *B, int i, const void *wavelet, int64_t nt)
+{
+    if (!B || i < 0 || i >= (int)B->solves.size()) return fail(PE_ERR_INVALID, "bad solve index");
+    return pe_solver_set_wavelet(B->solves[i], wavelet, nt);
+}
+
+int pe_batch_run(PeBatch *B, const PeState *states, void *const *traces, int64_t b, int64_t e, void *stream)
+{
+    if (!B || !states || !traces) return fail(PE_ERR_INVALID, "null argument");
+    if (b < 0 || e < b) return fail(PE_ERR_INVALID, "need 0 <= step_begin <= step_end");
+    for (int s = 0; s < (int)B->solves.size(); ++s) {
+        PeSolver *S = B->solves[s];
+        if (S->n_src > 0 && e > S->nt_wav) return fail(PE_ERR_INVALID, "solve " + std::to_string(s) + ": wavelet shorter than step_end");
+        if (S->n_groups > 0 && !traces[s]) return fail(PE_ERR_INVALID, "solve " + std::to_string(s) + ": traces buffer required");
+    }
+    B->launches = 0;
+    if (e == b) return PE_OK;
+    return B->dtype == PE_F64 ? batch_run_t<double>(B, states, traces, b, e, (cudaStream_t)stream)
+                              : batch_run_t<float>(B, states, traces, b, e, (cudaStream_t)stream);
+}
+
+int pe_batch_status(PeBatch *B)
+{
+    if (!B) return fail(PE_ERR_INVALID, "null batch");
+    int st = 0;
+    PE_CUDA(cudaStreamSynchronize(B->stream));
+    PE_CUDA(cudaMemcpy(&st, B->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+        PE_CUDA(cudaMemset(B->status, 0, sizeof(int)));
+        return fail(PE_ERR_TIMEOUT, "a bounded device-side wait gave up; the batch results are invalid");
+    }
+    return PE_OK;
+}
+
+int64_t pe_batch_launch_count(const PeBatch *B) { return B ? B->launches : -1; }
+
+int pe_batch_destroy(PeBatch *B)
+{
+    delete B;
+    return PE_OK;
+}
+
+}  // extern "C"

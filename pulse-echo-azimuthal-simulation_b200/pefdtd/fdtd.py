@@ -77,6 +77,67 @@ def _flat_probe(shape, src_pts, rec_groups, npdt):
     return s_idx, s_w, np.array(offs, np.int64), r_idx, r_w
 
 
+def c_solve_structs(mats, Ct, rho_t, h, dt, coeffs, src_idx, src_w, rec_off, rec_idx, rec_w,
+                    record="pressure", damped_record=False, sponge=None, damp_volume=None,
+                    dtype="float32", device=None, chunk_steps=0, tile=(0, 0), z_chunk=0,
+                    variant="tiled"):
+    """The C ABI description of one solve (PeConfig, PeMedium, PeProbe) plus
+    the host arrays and device tensors it points at, which must stay alive
+    until the solver has been created."""
+    torch = _torch()
+    npdt, pedt = _dtype(dtype)
+    mats = np.asarray(mats)
+    shape = tuple(int(v) for v in mats.shape)
+    nz, ny, nx = shape
+    coeffs = np.asarray(coeffs, float).reshape(-1)
+    if record not in _capi.REC_KIND:
+        raise ValueError(f"record must be one of {sorted(_capi.REC_KIND)}, got {record!r}")
+    if variant not in _capi.KERNEL_VARIANT:
+        raise ValueError(f"variant must be one of {sorted(_capi.KERNEL_VARIANT)}")
+    cfg = _capi.PeConfig()
+    cfg.nz, cfg.ny, cfg.nx = nz, ny, nx
+    cfg.dtype = pedt
+    cfg.n_coeffs = len(coeffs)
+    for j, c in enumerate(coeffs[:4]):
+        cfg.coeffs[j] = float(c)
+    cfg.h, cfg.dt = float(h), float(dt)
+    cfg.record = _capi.REC_KIND[record]
+    cfg.damped_record = int(bool(damped_record))
+    Ct = np.ascontiguousarray(np.asarray(Ct, npdt).reshape(-1, 36))
+    rho_t = np.ascontiguousarray(np.asarray(rho_t, npdt).reshape(-1))
+    cfg.n_mat = len(rho_t)
+    cfg.chunk_steps = int(chunk_steps)
+    cfg.tile_x, cfg.tile_y = int(tile[0]), int(tile[1])
+    cfg.z_chunk = int(z_chunk)
+    cfg.variant = _capi.KERNEL_VARIANT[variant]
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    with torch.cuda.device(dev):
+        lab_t = torch.from_numpy(np.ascontiguousarray(mats.astype(np.uint16).view(np.int16))).to(dev)
+        dvol_t = (torch.from_numpy(np.ascontiguousarray(damp_volume, np.float32)).to(dev)
+                  if damp_volume is not None else None)
+    keep = [lab_t, dvol_t, Ct, rho_t]
+    md = _capi.PeMedium()
+    md.labels_dev = lab_t.data_ptr()
+    md.damp_volume_dev = dvol_t.data_ptr() if dvol_t is not None else None
+    md.ctab, md.rho = _capi.ptr(Ct), _capi.ptr(rho_t)
+    if sponge is not None:
+        sp = [np.ascontiguousarray(p, np.float32) for p in sponge]
+        keep += sp
+        md.sponge_z, md.sponge_y, md.sponge_x = [_capi.ptr(p) for p in sp]
+    pr = _capi.PeProbe()
+    src_idx = np.ascontiguousarray(src_idx, np.int64)
+    src_w = np.ascontiguousarray(src_w, npdt)
+    rec_off = np.ascontiguousarray(rec_off, np.int64)
+    rec_idx = np.ascontiguousarray(rec_idx, np.int64)
+    rec_w = np.ascontiguousarray(rec_w, npdt)
+    keep += [src_idx, src_w, rec_off, rec_idx, rec_w]
+    pr.n_src = len(src_idx)
+    pr.src_idx, pr.src_w = _capi.ptr(src_idx), _capi.ptr(src_w)
+    pr.n_groups = len(rec_off) - 1
+    pr.rec_off, pr.rec_idx, pr.rec_w = _capi.ptr(rec_off), _capi.ptr(rec_idx), _capi.ptr(rec_w)
+    return dict(cfg=cfg, md=md, pr=pr, keep=keep, shape=shape, n_groups=len(rec_off) - 1)
+
+
 class DeviceSolve:
     """One solve held on the GPU: state, solver handle and trace buffer.
 
@@ -95,59 +156,16 @@ class DeviceSolve:
         self.tdt = torch.float64 if npdt == np.float64 else torch.float32
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
-        mats = np.asarray(mats)
-        self.shape = tuple(int(v) for v in mats.shape)
+        S = c_solve_structs(mats, Ct, rho_t, h, dt, coeffs, src_idx, src_w, rec_off, rec_idx, rec_w,
+                            record, damped_record, sponge, damp_volume, dtype, self.device,
+                            chunk_steps, tile, z_chunk, variant)
+        cfg, md, pr, keep = S["cfg"], S["md"], S["pr"], S["keep"]
+        self.shape = S["shape"]
         nz, ny, nx = self.shape
-        coeffs = np.asarray(coeffs, float).reshape(-1)
-        if record not in _capi.REC_KIND:
-            raise ValueError(f"record must be one of {sorted(_capi.REC_KIND)}, got {record!r}")
-        self.n_groups = len(rec_off) - 1
-        cfg = _capi.PeConfig()
-        cfg.nz, cfg.ny, cfg.nx = nz, ny, nx
-        cfg.dtype = pedt
-        cfg.n_coeffs = len(coeffs)
-        for j, c in enumerate(coeffs[:4]):
-            cfg.coeffs[j] = float(c)
-        cfg.h, cfg.dt = float(h), float(dt)
-        cfg.record = _capi.REC_KIND[record]
-        cfg.damped_record = int(bool(damped_record))
-        Ct = np.ascontiguousarray(np.asarray(Ct, npdt).reshape(-1, 36))
-        rho_t = np.ascontiguousarray(np.asarray(rho_t, npdt).reshape(-1))
-        cfg.n_mat = len(rho_t)
-        cfg.chunk_steps = int(chunk_steps)
-        cfg.tile_x, cfg.tile_y = int(tile[0]), int(tile[1])
-        cfg.z_chunk = int(z_chunk)
-        if variant not in _capi.KERNEL_VARIANT:
-            raise ValueError(f"variant must be one of {sorted(_capi.KERNEL_VARIANT)}")
-        cfg.variant = _capi.KERNEL_VARIANT[variant]
+        self.n_groups = S["n_groups"]
         self.cfg = cfg
         with torch.cuda.device(self.device):
-            self.lab_t = torch.from_numpy(np.ascontiguousarray(mats.astype(np.uint16).view(np.int16))
-                                          ).to(self.device)
-            self.dvol_t = (torch.from_numpy(np.ascontiguousarray(damp_volume, np.float32)).to(self.device)
-                           if damp_volume is not None else None)
             self.state = torch.zeros((9, nz, ny, nx), dtype=self.tdt, device=self.device)
-        keep = []
-        md = _capi.PeMedium()
-        md.labels_dev = self.lab_t.data_ptr()
-        md.damp_volume_dev = self.dvol_t.data_ptr() if self.dvol_t is not None else None
-        md.ctab, md.rho = _capi.ptr(Ct), _capi.ptr(rho_t)
-        keep += [Ct, rho_t]
-        if sponge is not None:
-            sp = [np.ascontiguousarray(p, np.float32) for p in sponge]
-            keep += sp
-            md.sponge_z, md.sponge_y, md.sponge_x = [_capi.ptr(p) for p in sp]
-        pr = _capi.PeProbe()
-        src_idx = np.ascontiguousarray(src_idx, np.int64)
-        src_w = np.ascontiguousarray(src_w, npdt)
-        rec_off = np.ascontiguousarray(rec_off, np.int64)
-        rec_idx = np.ascontiguousarray(rec_idx, np.int64)
-        rec_w = np.ascontiguousarray(rec_w, npdt)
-        keep += [src_idx, src_w, rec_off, rec_idx, rec_w]
-        pr.n_src = len(src_idx)
-        pr.src_idx, pr.src_w = _capi.ptr(src_idx), _capi.ptr(src_w)
-        pr.n_groups = self.n_groups
-        pr.rec_off, pr.rec_idx, pr.rec_w = _capi.ptr(rec_off), _capi.ptr(rec_idx), _capi.ptr(rec_w)
         L = _capi.lib()
         h_ = _capi.C.c_void_p()
         with torch.cuda.device(self.device):
