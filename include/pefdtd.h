@@ -201,6 +201,28 @@ int pe_label_cylinder(const double *xs, int nx, const double *ys, int ny, const 
                       int nz, double R2, const double *seeds, const double *weights, int ns,
                       int32_t *out_dev, void *stream);
 
+/* Allocation-free variant of pe_label_cylinder, with no counterpart in the
+ * reference. For callers that may not allocate device memory (an application
+ * whose framework has reserved the device pool for its own allocator, or a
+ * pipeline stage that must not pay cudaMalloc/cudaFree's implicit device
+ * synchronisation): the staged coordinates, seeds and weights go to a
+ * fixed-size file-scope device array instead of a cudaMalloc buffer, which
+ * every device that loads the library holds until exit
+ * (PE_NOALLOC_SCRATCH_BYTES). Same arguments and result as
+ * pe_label_cylinder; out_dev is still the caller's. Limits: nx + ny + nz <=
+ * PE_NOALLOC_MAX_COORDS and ns <= PE_NOALLOC_MAX_SEEDS, else PE_ERR_INVALID
+ * (message: pe_label_cylinder_noalloc_error). The first call on a device
+ * looks the array up (make it before any stream capture on that device). All
+ * calls on a device share the array: calls that can overlap on the GPU race
+ * and must be serialised by the caller. Synchronous on `stream`. */
+#define PE_NOALLOC_MAX_COORDS 12288
+#define PE_NOALLOC_MAX_SEEDS 16384
+#define PE_NOALLOC_SCRATCH_BYTES (8 * (PE_NOALLOC_MAX_COORDS + 4 * PE_NOALLOC_MAX_SEEDS))
+int pe_label_cylinder_noalloc(const double *xs, int nx, const double *ys, int ny, const double *zs,
+                              int nz, double R2, const double *seeds, const double *weights, int ns,
+                              int32_t *out_dev, void *stream);
+const char *pe_label_cylinder_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,3 +96,93 @@ extern "C" int pe_label_cylinder(const double *xs, int nx, const double *ys, int
     cudaFree(d);
     return e == cudaSuccess ? PE_OK : PE_ERR_CUDA;
 }
+
+// ------------------------------------------------------------------------------
+// Allocation-free variant of the labeller, for callers that may not allocate
+// device memory at all: a host application whose framework has reserved the
+// whole device pool for its own caching allocator, or a pipeline stage that
+// must not pay cudaMalloc/cudaFree's implicit device synchronisation in the
+// middle of an acquisition loop. The grid coordinates, seeds and weights that
+// pe_label_cylinder stages in a fresh cudaMalloc buffer are staged instead in
+// this file-scope device array. Every device that loads the library holds
+// the array (PE_NOALLOC_SCRATCH_BYTES) until the process exits.
+//
+// Contract:
+//  - limits: nx + ny + nz <= PE_NOALLOC_MAX_COORDS, ns <= PE_NOALLOC_MAX_SEEDS;
+//    larger requests return PE_ERR_INVALID with a message and touch nothing;
+//  - the first call on a device looks the array up (cudaGetSymbolAddress,
+//    with that device current) and caches the address; make that first call
+//    before any stream capture on the device;
+//  - all calls on a device share the one array and every call overwrites
+//    it (the weights are zeroed when none are given): calls that can overlap
+//    on the GPU (different streams, different host threads) race and must be
+//    serialised by the caller;
+//  - no cudaMalloc, cudaFree or other allocating routine is called.
+// ------------------------------------------------------------------------------
+namespace {
+
+constexpr int NOALLOC_MAX_COORDS = 12288;
+constexpr int NOALLOC_MAX_SEEDS = 16384;
+constexpr size_t NOALLOC_DOUBLES = (size_t)NOALLOC_MAX_COORDS + 4 * (size_t)NOALLOC_MAX_SEEDS;
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+thread_local std::string g_noalloc_err;
+
+int noalloc_fail(int code, const std::string &msg)
+{
+    g_noalloc_err = msg;
+    return code;
+}
+
+}  // namespace
+
+extern "C" const char *pe_label_cylinder_noalloc_error(void) { return g_noalloc_err.c_str(); }
+
+extern "C" int pe_label_cylinder_noalloc(const double *xs, int nx, const double *ys, int ny,
+                                         const double *zs, int nz, double R2, const double *seeds,
+                                         const double *weights, int ns, int32_t *out_dev, void *stream)
+{
+    if (!xs || !ys || !zs || !seeds || !out_dev || nx < 1 || ny < 1 || nz < 1 || ns < 1)
+        return noalloc_fail(PE_ERR_INVALID, "null pointer or empty axis / seed list");
+    if ((long long)nx + ny + nz > NOALLOC_MAX_COORDS)
+        return noalloc_fail(PE_ERR_INVALID, "nx + ny + nz = " + std::to_string((long long)nx + ny + nz) +
+                                                " exceeds the allocation-free limit of " +
+                                                std::to_string(NOALLOC_MAX_COORDS));
+    if (ns > NOALLOC_MAX_SEEDS)
+        return noalloc_fail(PE_ERR_INVALID, std::to_string(ns) + " seeds exceed the allocation-free limit of " +
+                                                std::to_string(NOALLOC_MAX_SEEDS));
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return noalloc_fail(PE_ERR_CUDA, "no usable current device");
+    if (!g_noalloc_ptr[dev]) {
+        double *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return noalloc_fail(PE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    double *d = g_noalloc_ptr[dev];
+    cudaStream_t st = (cudaStream_t)stream;
+    double *dx = d, *dy = dx + nx, *dz = dy + ny, *ds = d + NOALLOC_MAX_COORDS, *dw = ds + 3 * (size_t)ns;
+    cudaError_t e = cudaMemcpyAsync(dx, xs, sizeof(double) * nx, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dy, ys, sizeof(double) * ny, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, zs, sizeof(double) * nz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, seeds, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        if (weights) e = cudaMemcpyAsync(dw, weights, sizeof(double) * ns, cudaMemcpyHostToDevice, st);
+        else e = cudaMemsetAsync(dw, 0, sizeof(double) * ns, st);
+    }
+    if (e == cudaSuccess) {
+        const long long n = (long long)nx * ny * nz;
+        k_label_cylinder<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dx, dy, dz, nx, ny, nz, R2, ds, dw,
+                                                                     ns, out_dev);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return noalloc_fail(PE_ERR_CUDA, std::string("labelling failed: ") + cudaGetErrorString(e));
+    return PE_OK;
+}
