@@ -166,6 +166,29 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host,
                     const PeProbe *probe, const void *wavelet_host, int64_t nt,
                     void *traces_host);
 
+/* ---- Adjoint ---------------------------------------------------------------
+ * One reverse step of the exact discrete adjoint of pe_solver_run's step n
+ * (the reference's only FDTD adjoint is the order-2, undamped, cell-density
+ * vendor/ringfwi/elastic3d.py:348-463; this is the adjoint of the full
+ * scheme: order 2..8, face density, sponge and damping volume, deferred
+ * damping, every record kind). On entry lv, ls hold dJ/d(v^n, s^n) from the
+ * later steps; the call adds the trace adjoint residual[n][g] at the
+ * receivers, then transposes the velocity and stress updates, leaving
+ * dJ/d(v^{n-1}, s^{n-1}) and adding dJ/dC of this step to grad. v_prev must
+ * hold the forward velocity at the start of step n (the caller recomputes
+ * it from checkpoints). All pointers are device memory of the solver's dtype
+ * except grad (f64). Asynchronous on `stream`. */
+typedef struct PeAdjoint {
+    void *lv[3];             /* adjoint of vx, vy, vz */
+    void *ls[6];             /* adjoint of s1..s6 */
+    const void *v_prev[3];   /* forward v^{n-1} */
+    void *scratch;           /* 15 fields of (nz, ny, nx) */
+    double *grad;            /* (n_mat, 21) dJ/dC upper triangle, accumulated */
+} PeAdjoint;
+
+int pe_solver_adjoint_step(PeSolver *s, const PeAdjoint *adj, int64_t n, const void *residual,
+                           void *stream);
+
 /* ---- Batches: many independent solves advanced together ----------------
  * No counterpart in the reference, which runs one azimuth at a time in a
  * Python loop (sim/pipeline/sweep_runner.py:322-390); the closest precedent

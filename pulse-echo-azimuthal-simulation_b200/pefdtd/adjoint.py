@@ -1,0 +1,273 @@
+"""Gradients of trace misfits through the FDTD solver (hand-written adjoint).
+
+The reference's only FDTD gradient is ringfwi's order-2, undamped,
+cell-density adjoint that stores the whole velocity history
+(vendor/ringfwi/elastic3d.py:276-463), chained to per-voxel c-axis angles by
+vendor/ringfwi/axisfield.py:37-161. Here:
+
+* :class:`AdjointSolve` runs the production forward scheme on the GPU,
+  keeping full-state checkpoints every ``checkpoint_every`` steps in device
+  memory; the reverse sweep recomputes each segment from its checkpoint,
+  keeping that segment's velocity history, and applies the exact discrete
+  adjoint step (csrc/pe_adjoint.cuh) backwards through it, accumulating
+  dJ/dC for every material's 21 stiffness constants.
+* :class:`StiffnessTraces` is a ``torch.autograd.Function`` from the
+  per-material table ``(n_mat, 21)`` to the traces ``(nt, n_groups)``; its
+  backward is that adjoint with the incoming trace gradient as the adjoint
+  source, so any loss on the traces (``0.5*||tr - d||^2`` gives the
+  reference's misfit) differentiates through it.
+* :func:`ice_table21` builds that table differentiably from per-grain c-axis
+  angles (colatitude theta, azimuth phi; R = Rz(phi) Ry(theta), the
+  convention of vendor/ringfwi/axisfield.py:37-65 and cof.axes_from_params),
+  and :func:`fabric_axes` maps 3 fabric parameters to per-grain axes, so
+  gradients reach grain angles and fabric parameters through torch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from .fdtd import DeviceSolve, _torch
+from .materials import C21_INDEX, ICE, ti_stiffness_6
+
+
+class _PeAdjoint(C.Structure):
+    _fields_ = [("lv", C.c_void_p * 3), ("ls", C.c_void_p * 6), ("v_prev", C.c_void_p * 3),
+                ("scratch", C.c_void_p), ("grad", C.c_void_p)]
+
+
+def _bind():
+    L = _capi.lib()
+    if not getattr(L, "_adj_bound", False):
+        L.pe_solver_adjoint_step.argtypes = [C.c_void_p, C.POINTER(_PeAdjoint), C.c_int64, C.c_void_p,
+                                             C.c_void_p]
+        L._adj_bound = True
+    return L
+
+
+class AdjointSolve:
+    """Forward with checkpoints, then reverse sweeps, on one DeviceSolve."""
+
+    def __init__(self, solve: DeviceSolve, checkpoint_every=200):
+        self.solve = solve
+        self.K = int(checkpoint_every)
+        if self.K < 1:
+            raise ValueError("checkpoint_every must be >= 1")
+        self.torch = solve.torch
+        self.ckpt = {}
+        self.nt = 0
+
+    def forward(self, nt=None):
+        """Traces (nt, n_groups) as a device tensor; keeps checkpoints."""
+        s = self.solve
+        nt = s.nt if nt is None else int(nt)
+        s.reset()
+        self.ckpt = {}
+        for a in range(0, nt, self.K):
+            self.ckpt[a] = s.state.clone()
+            s.run(a, min(a + self.K, nt))
+        self.nt = nt
+        s.check_status()
+        return s.traces[:nt, :s.n_groups]
+
+    def backward(self, residual):
+        """dJ/dC (n_mat, 21) float64 for the trace adjoint `residual`
+        (nt, n_groups): for J = 0.5 ||traces - d||^2 it is traces - d."""
+        torch = self.torch
+        s = self.solve
+        nt, ng = self.nt, s.n_groups
+        dev, tdt = s.device, s.tdt
+        shape = s.shape
+        res = torch.as_tensor(np.asarray(residual), dtype=tdt).reshape(nt, ng).to(dev).contiguous()
+        L = _bind()
+        with torch.cuda.device(dev):
+            lam = torch.zeros((9,) + shape, dtype=tdt, device=dev)
+            scratch = torch.zeros((15,) + shape, dtype=tdt, device=dev)
+            grad = torch.zeros((s.cfg.n_mat, 21), dtype=torch.float64, device=dev)
+            hist = torch.empty((min(self.K, nt), 3) + shape, dtype=tdt, device=dev)
+        adj = _PeAdjoint()
+        for i in range(3):
+            adj.lv[i] = lam[i].data_ptr()
+        for i in range(6):
+            adj.ls[i] = lam[3 + i].data_ptr()
+        adj.scratch = scratch.data_ptr()
+        adj.grad = grad.data_ptr()
+        stream = torch.cuda.current_stream(dev)
+        starts = sorted(self.ckpt)
+        for a in reversed(starts):
+            b = min(a + self.K, nt)
+            s.state.copy_(self.ckpt[a])
+            for n in range(a, b):
+                hist[n - a].copy_(s.state[:3])
+                s.run(n, n + 1)
+            for n in range(b - 1, a - 1, -1):
+                for i in range(3):
+                    adj.v_prev[i] = hist[n - a, i].data_ptr()
+                with torch.cuda.device(dev):
+                    _capi.check(L.pe_solver_adjoint_step(s._h, C.byref(adj), n, res.data_ptr(),
+                                                         C.c_void_p(stream.cuda_stream)))
+        s.check_status()
+        return grad.cpu().numpy()
+
+
+# ---------------------------------------------------------------- autograd
+class StiffnessTraces:
+    """Namespace for the autograd Function (created lazily so that importing
+    this module does not require torch)."""
+    _fn = None
+
+    @classmethod
+    def fn(cls):
+        if cls._fn is None:
+            torch = _torch()
+
+            class _F(torch.autograd.Function):
+                @staticmethod
+                def forward(ctx, c21, problem):
+                    adj = problem.make_adjoint(c21.detach().cpu().numpy())
+                    tr = adj.forward()
+                    ctx.adj = adj
+                    return tr.detach().to("cpu", torch.float64)
+
+                @staticmethod
+                def backward(ctx, grad_tr):
+                    g = ctx.adj.backward(grad_tr.detach().cpu().numpy())
+                    ctx.adj.solve.close()
+                    return torch.from_numpy(g), None
+
+            cls._fn = _F
+        return cls._fn
+
+
+class Problem:
+    """Everything of a solve except the stiffness table: labels, densities,
+    probe, wavelet, damping and scheme. ``traces(c21)`` is differentiable in
+    ``c21`` (torch tensor (n_mat, 21))."""
+
+    def __init__(self, mats, rho_t, h, dt, coeffs, src_pts, rec_groups, wavelet, record="vz",
+                 sponge_width=0, damp_mask=None, damped_record=True, dtype="float64",
+                 checkpoint_every=200, device=None):
+        from .damping import sponge_axis_profiles
+        from .fdtd import _flat_probe
+        self.mats = np.asarray(mats)
+        self.rho_t = np.asarray(rho_t, float)
+        self.h, self.dt = float(h), float(dt)
+        self.coeffs = np.asarray(coeffs, float)
+        shape = self.mats.shape
+        self.probe = _flat_probe(shape, src_pts, rec_groups, np.float64)
+        self.wavelet = np.asarray(wavelet, float)
+        self.record = record
+        self.sponge = sponge_axis_profiles(shape, sponge_width) if sponge_width > 0 else None
+        self.damp_mask = damp_mask
+        self.damped_record = damped_record
+        self.dtype = dtype
+        self.K = checkpoint_every
+        self.device = device
+
+    def make_adjoint(self, c21):
+        c21 = np.asarray(c21, float).reshape(-1, 21)
+        Ct = np.zeros((len(c21), 6, 6))
+        for k, (i, j) in enumerate(C21_INDEX):
+            Ct[:, i, j] = c21[:, k]
+            Ct[:, j, i] = c21[:, k]
+        s_idx, s_w, r_off, r_idx, r_w = self.probe
+        solve = DeviceSolve(self.mats, Ct.reshape(-1, 36), self.rho_t, self.h, self.dt, self.coeffs,
+                            s_idx, s_w, r_off, r_idx, r_w, record=self.record,
+                            damped_record=self.damped_record, sponge=self.sponge,
+                            damp_volume=self.damp_mask, dtype=self.dtype, device=self.device)
+        solve.set_wavelet(self.wavelet)
+        return AdjointSolve(solve, self.K)
+
+    def traces(self, c21):
+        return StiffnessTraces.fn().apply(c21, self)
+
+
+# ---------------------------------------------------------------- tables from angles
+def _bond_torch(A, B):
+    """Bilinear Bond form for (P,3,3) tensors; _bond_torch(R, R) = M(R)."""
+    torch = _torch()
+    V = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))
+    rows = []
+    for (i, j) in V:
+        cols = []
+        for (k, l) in V:
+            v = A[:, i, k] * B[:, j, l]
+            if k != l:
+                v = v + A[:, i, l] * B[:, j, k]
+            cols.append(v)
+        rows.append(torch.stack(cols, dim=-1))
+    return torch.stack(rows, dim=-2)
+
+
+def rotation_colat_azim(theta, phi):
+    """R = Rz(phi) Ry(theta): maps the crystal c-axis z onto
+    (sin t cos p, sin t sin p, cos t)."""
+    torch = _torch()
+    ct, st, cp, sp = torch.cos(theta), torch.sin(theta), torch.cos(phi), torch.sin(phi)
+    z, o = torch.zeros_like(theta), torch.ones_like(theta)
+    Ry = torch.stack([torch.stack([ct, z, st], -1), torch.stack([z, o, z], -1),
+                      torch.stack([-st, z, ct], -1)], -2)
+    Rz = torch.stack([torch.stack([cp, -sp, z], -1), torch.stack([sp, cp, z], -1),
+                      torch.stack([z, z, o], -1)], -2)
+    return Rz @ Ry
+
+
+def ice_table21(theta, phi, c_couplant=1500.0, rho_couplant=300.0, material=None):
+    """(n_g + 1, 21) stiffness table (row 0 the fluid couplant) from per-grain
+    c-axis angles, differentiable in theta and phi (torch float64)."""
+    torch = _torch()
+    mat = ICE if material is None else material
+    theta = torch.as_tensor(theta, dtype=torch.float64)
+    phi = torch.as_tensor(phi, dtype=torch.float64)
+    R = rotation_colat_azim(theta, phi)
+    M = _bond_torch(R, R)
+    C0 = torch.as_tensor(ti_stiffness_6(**mat), dtype=torch.float64)
+    Cg = M @ C0 @ M.transpose(-1, -2)
+    iu = [i for i, _ in C21_INDEX], [j for _, j in C21_INDEX]
+    g21 = Cg[:, iu[0], iu[1]]
+    K = rho_couplant * c_couplant * c_couplant
+    fl = torch.zeros(1, 21, dtype=torch.float64)
+    for k, (i, j) in enumerate(C21_INDEX):
+        if i < 3 and j < 3:
+            fl[0, k] = K
+    return torch.cat([fl, g21], dim=0)
+
+
+def angles_from_axes(axes):
+    """(theta, phi) of unit axes (upper hemisphere; c and -c are the same)."""
+    a = np.asarray(axes, float).reshape(-1, 3)
+    a = np.where(a[:, 2:3] < 0, -a, a)
+    theta = np.arccos(np.clip(a[:, 2], -1, 1))
+    phi = np.arctan2(a[:, 1], a[:, 0])
+    return theta, phi
+
+
+def fabric_axes(params, base):
+    """Per-grain c-axes from 3 fabric parameters (tilt, azimuth, log_conc)
+    and fixed per-grain base directions (n, 3): each base direction is
+    stretched by exp(log_conc) along z (> 0 clusters the axes about the pole,
+    < 0 spreads them toward a girdle), normalised, then the whole fabric is
+    tilted by `tilt` about y and turned by `azimuth` about z. Differentiable;
+    a construction of this module (the reference's fabric fits use Watson
+    (alpha, kappa) on ray-model observables, sim/model/fit_fabric.py:224-274).
+    """
+    torch = _torch()
+    p = torch.as_tensor(params, dtype=torch.float64)
+    u = torch.as_tensor(base, dtype=torch.float64)
+    s = torch.exp(p[2])
+    a = torch.stack([u[:, 0], u[:, 1], u[:, 2] * s], -1)
+    a = a / torch.linalg.norm(a, dim=-1, keepdim=True)
+    R = rotation_colat_azim(p[0].reshape(1), p[1].reshape(1))[0]
+    return a @ R.T
+
+
+def theta_phi_torch(axes):
+    torch = _torch()
+    z = axes[:, 2]
+    sgn = torch.where(z < 0, -torch.ones_like(z), torch.ones_like(z))
+    a = axes * sgn[:, None]
+    theta = torch.acos(torch.clamp(a[:, 2], -1.0, 1.0))
+    phi = torch.atan2(a[:, 1], a[:, 0])
+    return theta, phi

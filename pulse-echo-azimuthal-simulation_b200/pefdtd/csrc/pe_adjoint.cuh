@@ -1,0 +1,353 @@
+// Discrete adjoint (reverse-time) step of the label-indexed elastic FDTD.
+//
+// The forward step n maps (v^{n-1}, s^{n-1}) to (v^n, s^n):
+//   g   = D v^{n-1}                       strains (order-2..8 staggered taps)
+//   s^n = d s^{n-1} + dt C(M g) + src     stress (half-cell moves M, 6x6 C)
+//   v^n = d (v^{n-1} + dt_h G(s^n) / rho_face)
+// and the recorded samples are linear in (v^n, s^n). These kernels apply the
+// exact transpose of that map, in reverse order, to the adjoint state
+// (lv, ls) = dJ/d(v^n, s^n), and accumulate dJ/dC per material:
+//   k_adj_inject    lv or ls += trace adjoint at the receiver cells
+//   k_adj_vel_u     u = d dt_h lv / rho_face              (per component)
+//   k_adj_vel       ls += G^T u                           (gathers)
+//   k_adj_strain    g = D v^{n-1}                         (same taps as forward)
+//   k_adj_stress    dJ/dC[m] += dt ls (x) (M g); t = M^T C^T (dt ls)
+//   k_adj_velfin    lv = d lv + D^T t
+//   k_adj_damp      ls = d ls
+// Every transpose is a gather that evaluates the forward guard at the forward
+// cell it reads from, so the boundaries transpose exactly and no result
+// depends on thread order except the per-material gradient sums (f64
+// atomics after warp aggregation). The reference's own adjoint is the
+// order-2, cell-density, undamped vendor/ringfwi/elastic3d.py:348-463; this
+// one is the adjoint of the full production scheme.
+#pragma once
+#include "pe_kernels.cuh"
+
+namespace pe {
+
+template <typename T>
+struct AdjArgs {
+    T *lv[3];          // adjoint of v
+    T *ls[6];          // adjoint of s
+    const T *vp[3];    // forward v at the start of the step (v^{n-1})
+    T *u[3];           // scratch: scaled velocity adjoint
+    T *g[6];           // scratch: forward strains
+    T *t[6];           // scratch: strain adjoint
+    const uint16_t *lab;
+    const T *c21;      // (n_mat, C21_STRIDE)
+    const T *rho;
+    const float *dz, *dy, *dx, *dvol;
+    int nz, ny, nx;
+    long long sy, sz;
+    T c[4];
+    int nc;
+    T inv_h, dt, dt_h;
+    double *grad;      // (n_mat, 21) dJ/dC, upper triangle row major
+};
+
+__device__ __forceinline__ bool gF(int x, int j, int n) { return x >= j && x < n - j - 1; }
+__device__ __forceinline__ bool gB(int x, int j, int n) { return x >= j + 1 && x < n - j; }
+
+template <typename T>
+__device__ __forceinline__ float adj_damp(const AdjArgs<T> &A, int iz, int iy, int ix, long long idx)
+{
+    float d = 1.0f;
+    if (A.dz) {
+        d = A.dz[iz] * A.dy[iy];
+        d = d * A.dx[ix];
+    }
+    if (A.dvol) d = A.dz ? d * A.dvol[idx] : A.dvol[idx];
+    return d;
+}
+
+// transpose of the forward derivative along one axis, at position y of an
+// axis of length n; f(o) reads the operand at y + o (only called where the
+// forward cell y + o exists)
+template <typename T, typename F>
+__device__ __forceinline__ T DfT(const F &f, int y, int n, const T c[4], int nc)
+{
+    T a = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (j < nc) {
+            if (gF(y - j - 1, j, n)) a += c[j] * f(-j - 1);
+            if (gF(y + j, j, n)) a -= c[j] * f(j);
+        }
+    }
+    return a;
+}
+template <typename T, typename F>
+__device__ __forceinline__ T DbT(const F &f, int y, int n, const T c[4], int nc)
+{
+    T a = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (j < nc) {
+            if (gB(y - j, j, n)) a += c[j] * f(-j);
+            if (gB(y + j + 1, j, n)) a -= c[j] * f(j + 1);
+        }
+    }
+    return a;
+}
+
+template <typename T>
+__device__ __forceinline__ void cell_of(const AdjArgs<T> &A, long long i, int &iz, int &iy, int &ix)
+{
+    ix = (int)(i % A.nx);
+    iy = (int)((i / A.nx) % A.ny);
+    iz = (int)(i / ((long long)A.nx * A.ny));
+}
+
+// ---------------------------------------------------------------- receivers
+// entries: cells[k] sorted, pos[k] = caller position; w and grp in caller order
+template <typename T>
+__global__ void k_adj_inject(AdjArgs<T> A, const long long *cells, const int *pos, const T *w,
+                             const int *grp, int n_ent, const T *res_row, int kind, int damped)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_ent) return;
+    const long long q = cells[k];
+    const int e = pos[k];
+    const T val = res_row[grp[e]] * w[e];
+    if (kind == 0) {
+        T f = -val / T(3);
+        if (damped) {
+            int iz, iy, ix;
+            cell_of(A, q, iz, iy, ix);
+            f = f * (T)adj_damp(A, iz, iy, ix, q);
+        }
+        atomicAdd(A.ls[0] + q, f);
+        atomicAdd(A.ls[1] + q, f);
+        atomicAdd(A.ls[2] + q, f);
+    } else {
+        atomicAdd(A.lv[kind - 1] + q, val);
+    }
+}
+
+// ---------------------------------------------------------------- velocity transpose
+template <typename T>
+__global__ void k_adj_vel_u(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    int iz, iy, ix;
+    cell_of(A, i, iz, iy, ix);
+    const T r0 = A.rho[A.lab[i] & LAB_MAT];
+    const T rvx = ix < A.nx - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + 1] & LAB_MAT]) : r0;
+    const T rvy = iy < A.ny - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + A.sy] & LAB_MAT]) : r0;
+    const T rvz = iz < A.nz - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + A.sz] & LAB_MAT]) : r0;
+    const T s = (T)adj_damp(A, iz, iy, ix, i) * A.dt_h;
+    A.u[0][i] = s * A.lv[0][i] / rvx;
+    A.u[1][i] = s * A.lv[1][i] / rvy;
+    A.u[2][i] = s * A.lv[2][i] / rvz;
+}
+
+template <typename T>
+__global__ void k_adj_vel(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    int iz, iy, ix;
+    cell_of(A, i, iz, iy, ix);
+    const long long sy = A.sy, sz = A.sz;
+    const T *ux = A.u[0] + i, *uy = A.u[1] + i, *uz = A.u[2] + i;
+    auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
+    auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
+    auto Z = [&](const T *p) { return [p, sz](int o) { return p[o * sz]; }; };
+    A.ls[0][i] += DfT<T>(X(ux), ix, A.nx, A.c, A.nc);
+    A.ls[1][i] += DfT<T>(Y(uy), iy, A.ny, A.c, A.nc);
+    A.ls[2][i] += DfT<T>(Z(uz), iz, A.nz, A.c, A.nc);
+    A.ls[3][i] += DbT<T>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T>(Y(uz), iy, A.ny, A.c, A.nc);
+    A.ls[4][i] += DbT<T>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T>(X(uz), ix, A.nx, A.c, A.nc);
+    A.ls[5][i] += DbT<T>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T>(X(uy), ix, A.nx, A.c, A.nc);
+}
+
+// ---------------------------------------------------------------- strains of v^{n-1}
+template <typename T>
+__global__ void k_adj_strain(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    int iz, iy, ix;
+    cell_of(A, i, iz, iy, ix);
+    const long long sy = A.sy, sz = A.sz;
+    const T *vx = A.vp[0], *vy = A.vp[1], *vz = A.vp[2];
+    T a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (j < A.nc) {
+            const T cj = A.c[j];
+            if (gB(ix, j, A.nx)) a1 = fmac(a1, cj, vx[i + j] - vx[i - (j + 1)]);
+            if (gB(iy, j, A.ny)) a2 = fmac(a2, cj, vy[i + j * sy] - vy[i - (j + 1) * sy]);
+            if (gB(iz, j, A.nz)) a3 = fmac(a3, cj, vz[i + j * sz] - vz[i - (j + 1) * sz]);
+            if (gF(iy, j, A.ny)) a4 = fmac(a4, cj, vz[i + (j + 1) * sy] - vz[i - j * sy]);
+            if (gF(iz, j, A.nz)) a4 = fmac(a4, cj, vy[i + (j + 1) * sz] - vy[i - j * sz]);
+            if (gF(ix, j, A.nx)) a5 = fmac(a5, cj, vz[i + (j + 1)] - vz[i - j]);
+            if (gF(iz, j, A.nz)) a5 = fmac(a5, cj, vx[i + (j + 1) * sz] - vx[i - j * sz]);
+            if (gF(ix, j, A.nx)) a6 = fmac(a6, cj, vy[i + (j + 1)] - vy[i - j]);
+            if (gF(iy, j, A.ny)) a6 = fmac(a6, cj, vx[i + (j + 1) * sy] - vx[i - j * sy]);
+        }
+    }
+    const T ih = A.inv_h;
+    A.g[0][i] = a1 * ih; A.g[1][i] = a2 * ih; A.g[2][i] = a3 * ih;
+    A.g[3][i] = a4 * ih; A.g[4][i] = a5 * ih; A.g[5][i] = a6 * ih;
+}
+
+// move guard at forward cell (z, y, x) for offsets d (exactly the forward's)
+__device__ __forceinline__ bool move_ok(int z, int y, int x, int dz, int dy, int dx, int nz, int ny, int nx)
+{
+    if (z < 0 || z >= nz || y < 0 || y >= ny || x < 0 || x >= nx) return false;
+    if (dz > 0 && z > nz - 2) return false;
+    if (dz < 0 && z < 1) return false;
+    if (dy > 0 && y > ny - 2) return false;
+    if (dy < 0 && y < 1) return false;
+    if (dx > 0 && x > nx - 2) return false;
+    if (dx < 0 && x < 1) return false;
+    return true;
+}
+
+// ---------------------------------------------------------------- stress transpose
+template <typename T>
+__global__ void k_adj_stress(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < (long long)A.nz * A.ny * A.nx;
+    int iz = 0, iy = 0, ix = 0;
+    if (live) cell_of(A, i, iz, iy, ix);
+    const int nz = A.nz, ny = A.ny, nx = A.nx;
+    const long long sy = A.sy, sz = A.sz;
+    const int POSZ[4] = {0, 1, 1, 0}, POSY[4] = {0, 1, 0, 1}, POSX[4] = {0, 0, 1, 1};
+    const int VP[6] = {0, 0, 0, 1, 2, 3};
+    double gsum[21];
+#pragma unroll
+    for (int k = 0; k < 21; ++k) gsum[k] = 0.0;
+    int m = 0;
+    if (live) {
+        m = A.lab[i] & LAB_MAT;
+        const T *Cm = A.c21 + (long long)m * C21_STRIDE;
+        T e[6];
+#pragma unroll
+        for (int I = 0; I < 6; ++I) e[I] = A.dt * A.ls[I][i];
+        // moved strains at this cell, q[p][J]
+        T q[4][6];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int J = 0; J < 6; ++J) {
+                const int s = VP[J];
+                const int dz = POSZ[p] - POSZ[s], dy = POSY[p] - POSY[s], dx = POSX[p] - POSX[s];
+                if (dz == 0 && dy == 0 && dx == 0) {
+                    q[p][J] = A.g[J][i];
+                } else if (!move_ok(iz, iy, ix, dz, dy, dx, nz, ny, nx)) {
+                    q[p][J] = 0;
+                } else {
+                    T acc = 0;
+                    for (int a0 = (dz < 0 ? -1 : 0); a0 <= (dz > 0 ? 1 : 0); ++a0)
+                        for (int a1 = (dy < 0 ? -1 : 0); a1 <= (dy > 0 ? 1 : 0); ++a1)
+                            for (int a2 = (dx < 0 ? -1 : 0); a2 <= (dx > 0 ? 1 : 0); ++a2)
+                                acc += A.g[J][i + a0 * sz + a1 * sy + a2];
+                    q[p][J] = acc * T(0.25);
+                }
+            }
+        // dJ/dC_IJ for I <= J: e_I q[p(I)][J] + e_J q[p(J)][I]  (I != J)
+#pragma unroll
+        for (int I = 0; I < 6; ++I)
+#pragma unroll
+            for (int J = I; J < 6; ++J) {
+                double v = (double)e[I] * (double)q[VP[I]][J];
+                if (J != I) v += (double)e[J] * (double)q[VP[J]][I];
+                gsum[c21_slot(I, J)] = v;
+            }
+        // strain adjoint t_J: direct term plus transposed moves of
+        // W[p][J](x) = sum_{I at p} C_IJ(x) e_I(x) from the forward cells x
+        T tJ[6];
+#pragma unroll
+        for (int J = 0; J < 6; ++J) {
+            const int s = VP[J];
+            T acc = 0;
+            for (int p = 0; p < 4; ++p) {
+                const int dz = POSZ[p] - POSZ[s], dy = POSY[p] - POSY[s], dx = POSX[p] - POSX[s];
+                if (dz == 0 && dy == 0 && dx == 0) {
+                    for (int I = 0; I < 6; ++I)
+                        if (VP[I] == p) acc += Cm[c21_slot(I, J)] * e[I];
+                    continue;
+                }
+                // forward cells x = y - o for every tap offset o of this move
+                for (int a0 = (dz < 0 ? -1 : 0); a0 <= (dz > 0 ? 1 : 0); ++a0)
+                    for (int a1 = (dy < 0 ? -1 : 0); a1 <= (dy > 0 ? 1 : 0); ++a1)
+                        for (int a2 = (dx < 0 ? -1 : 0); a2 <= (dx > 0 ? 1 : 0); ++a2) {
+                            const int xz = iz - a0, xy = iy - a1, xx = ix - a2;
+                            if (!move_ok(xz, xy, xx, dz, dy, dx, nz, ny, nx)) continue;
+                            const long long xi = i - a0 * sz - a1 * sy - a2;
+                            const T *Cx = A.c21 + (long long)(A.lab[xi] & LAB_MAT) * C21_STRIDE;
+                            T W = 0;
+                            for (int I = 0; I < 6; ++I)
+                                if (VP[I] == p) W += Cx[c21_slot(I, J)] * (A.dt * A.ls[I][xi]);
+                            acc += T(0.25) * W;
+                        }
+            }
+            tJ[J] = acc;
+        }
+#pragma unroll
+        for (int J = 0; J < 6; ++J) A.t[J][i] = tJ[J];
+    }
+    // per-material gradient: one full-warp butterfly per distinct material in
+    // the warp (lanes of other materials contribute zero), then one f64
+    // atomic per material and constant; every lane of the warp takes part
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int my = live ? m : -1;
+    unsigned remaining = __ballot_sync(full, live);
+    while (remaining) {
+        const int src = __ffs(remaining) - 1;
+        const int mm = __shfl_sync(full, my, src);
+        remaining &= ~__ballot_sync(full, my == mm);
+#pragma unroll
+        for (int k = 0; k < 21; ++k) {
+            double v = my == mm ? gsum[k] : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(full, v, off);
+            if (lane == src) atomicAdd(A.grad + (long long)mm * 21 + k, v);
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_adj_velfin(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    int iz, iy, ix;
+    cell_of(A, i, iz, iy, ix);
+    const long long sy = A.sy, sz = A.sz;
+    auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
+    auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
+    auto Z = [&](const T *p) { return [p, sz](int o) { return p[o * sz]; }; };
+    const T *t1 = A.t[0] + i, *t2 = A.t[1] + i, *t3 = A.t[2] + i;
+    const T *t4 = A.t[3] + i, *t5 = A.t[4] + i, *t6 = A.t[5] + i;
+    const T d = (T)adj_damp(A, iz, iy, ix, i);
+    const T ih = A.inv_h;
+    const T gx = DbT<T>(X(t1), ix, A.nx, A.c, A.nc) + DfT<T>(Z(t5), iz, A.nz, A.c, A.nc) +
+                 DfT<T>(Y(t6), iy, A.ny, A.c, A.nc);
+    const T gy = DbT<T>(Y(t2), iy, A.ny, A.c, A.nc) + DfT<T>(Z(t4), iz, A.nz, A.c, A.nc) +
+                 DfT<T>(X(t6), ix, A.nx, A.c, A.nc);
+    const T gz = DbT<T>(Z(t3), iz, A.nz, A.c, A.nc) + DfT<T>(Y(t4), iy, A.ny, A.c, A.nc) +
+                 DfT<T>(X(t5), ix, A.nx, A.c, A.nc);
+    A.lv[0][i] = d * A.lv[0][i] + ih * gx;
+    A.lv[1][i] = d * A.lv[1][i] + ih * gy;
+    A.lv[2][i] = d * A.lv[2][i] + ih * gz;
+}
+
+template <typename T>
+__global__ void k_adj_damp(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    int iz, iy, ix;
+    cell_of(A, i, iz, iy, ix);
+    const T d = (T)adj_damp(A, iz, iy, ix, i);
+#pragma unroll
+    for (int I = 0; I < 6; ++I) A.ls[I][i] = d * A.ls[I][i];
+}
+
+}  // namespace pe

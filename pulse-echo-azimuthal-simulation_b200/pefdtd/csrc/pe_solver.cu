@@ -19,6 +19,7 @@
 #include "pe_kernels.cuh"
 #include "pe_kernels_tiled.cuh"
 #include "pe_kernels_tma.cuh"
+#include "pe_adjoint.cuh"
 #include "pefdtd.h"
 
 namespace {
@@ -74,6 +75,7 @@ struct PeSolver {
     int *rec_pos = nullptr;
     void *rec_w = nullptr;
     long long *grp_off = nullptr;
+    int *ent_group = nullptr;   // group of each receiver entry (caller order)
     int n_rec = 0, n_groups = 0;
     void *rec_val = nullptr;
     void *wavelet = nullptr;
@@ -105,7 +107,7 @@ struct PeSolver {
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
         void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
-                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status};
+                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group};
         for (void *b : bufs)
             if (b) cudaFree(b);
     }
@@ -577,6 +579,14 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     }
     if (S->n_groups > 0)
         PE_CUDA(cudaMemcpyAsync(S->grp_off, roff.data(), sizeof(long long) * (S->n_groups + 1), cudaMemcpyHostToDevice, st));
+    {
+        std::vector<int> eg((size_t)std::max<long long>(1, n_rec), 0);
+        for (int g = 0; g < S->n_groups; ++g)
+            for (long long e = roff[g]; e < roff[g + 1]; ++e) eg[(size_t)e] = g;
+        if ((rc = dev_alloc(&S->ent_group, sizeof(int) * eg.size()))) return rc;
+        PE_CUDA(cudaMemcpyAsync(S->ent_group, eg.data(), sizeof(int) * eg.size(), cudaMemcpyHostToDevice, st));
+        PE_CUDA(cudaStreamSynchronize(st));
+    }
     PE_CUDA(cudaStreamSynchronize(st));
     PE_CUDA(cudaGetLastError());
     *out = S.release();
@@ -660,6 +670,78 @@ int pe_solver_run(PeSolver *S, const PeState *state, void *traces, int64_t b, in
 }
 
 int64_t pe_solver_launch_count(const PeSolver *S) { return S ? S->launches : -1; }
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *residual, cudaStream_t st)
+{
+    const PeConfig &c = S->cfg;
+    pe::AdjArgs<T> A{};
+    const long long ncell = S->ncell;
+    for (int i = 0; i < 3; ++i) {
+        A.lv[i] = (T *)adj->lv[i];
+        A.vp[i] = (const T *)adj->v_prev[i];
+        A.u[i] = (T *)adj->scratch + (size_t)i * ncell;
+    }
+    for (int i = 0; i < 6; ++i) {
+        A.ls[i] = (T *)adj->ls[i];
+        A.g[i] = (T *)adj->scratch + (size_t)(3 + i) * ncell;
+        A.t[i] = (T *)adj->scratch + (size_t)(9 + i) * ncell;
+    }
+    A.lab = S->lab;
+    A.c21 = (const T *)S->c21;
+    A.rho = (const T *)S->rho;
+    A.dz = S->dz;
+    A.dy = S->dy;
+    A.dx = S->dx;
+    A.dvol = S->dvol;
+    A.nz = c.nz;
+    A.ny = c.ny;
+    A.nx = c.nx;
+    A.sy = c.nx;
+    A.sz = (long long)c.nx * c.ny;
+    for (int j = 0; j < 4; ++j) A.c[j] = j < c.n_coeffs ? (T)c.coeffs[j] : T(0);
+    A.nc = c.n_coeffs;
+    A.inv_h = (T)(1.0 / c.h);
+    A.dt = (T)c.dt;
+    A.dt_h = (T)(c.dt / c.h);
+    A.grad = adj->grad;
+    const unsigned nb = (unsigned)((ncell + 255) / 256);
+    if (S->n_rec > 0 && residual) {
+        const T *row = (const T *)residual + (size_t)n * S->n_groups;
+        pe::k_adj_inject<T><<<(S->n_rec + 127) / 128, 128, 0, st>>>(A, S->rec_cell, S->rec_pos, (const T *)S->rec_w,
+                                                                     S->ent_group, S->n_rec, row, c.record,
+                                                                     c.damped_record);
+    }
+    pe::k_adj_vel_u<T><<<nb, 256, 0, st>>>(A);
+    pe::k_adj_vel<T><<<nb, 256, 0, st>>>(A);
+    pe::k_adj_strain<T><<<nb, 256, 0, st>>>(A);
+    pe::k_adj_stress<T><<<nb, 256, 0, st>>>(A);
+    pe::k_adj_velfin<T><<<nb, 256, 0, st>>>(A);
+    pe::k_adj_damp<T><<<nb, 256, 0, st>>>(A);
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pe_solver_adjoint_step(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *residual, void *stream)
+{
+    if (!S || !adj || !adj->scratch || !adj->grad) return fail(PE_ERR_INVALID, "null adjoint argument");
+    for (int i = 0; i < 3; ++i)
+        if (!adj->lv[i] || !adj->v_prev[i]) return fail(PE_ERR_INVALID, "adjoint velocity buffers missing");
+    for (int i = 0; i < 6; ++i)
+        if (!adj->ls[i]) return fail(PE_ERR_INVALID, "adjoint stress buffers missing");
+    if (n < 0) return fail(PE_ERR_INVALID, "negative step");
+    cudaStream_t st = (cudaStream_t)stream;
+    return S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, adj, n, residual, st)
+                                  : adjoint_step_t<float>(S, adj, n, residual, st);
+}
 
 int pe_solver_status(PeSolver *S)
 {

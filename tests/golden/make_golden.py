@@ -138,7 +138,69 @@ def main():
         res[f"{record}_f64"] = tr64
         res[f"{record}_f32"] = tr32
     np.savez_compressed(os.path.join(HERE, "forward_small.npz"), **res)
+    adjoint_compat()
     print("golden fixtures written to", HERE)
+
+
+def adjoint_compat():
+    """The reference's own gradient (vendor/ringfwi/axisfield.py:123-161 over
+    vendor/ringfwi/elastic3d.py:348-463) on a small matched problem: order 2,
+    no damping, pressure record, uniform density 917 (so face and cell
+    density agree), explosive source, one receiver group. Stores the inputs,
+    the observed traces, J and the per-grain (colatitude, azimuth) gradients
+    (per-voxel gradients summed over each grain)."""
+    from ringfwi import anisotropy as an
+    from ringfwi import axisfield as af
+    from ringfwi import elastic3d as e3
+    sys.path.insert(0, os.path.dirname(HERE))
+    from helpers import make_small
+    p = make_small(nt=60, shape=(16, 20, 20), n_grains=6, sponge=0, seed=3)
+    lab = p["lab"]
+    n_g = int(lab.max()) + 1
+    rng = np.random.default_rng(5)
+    theta = rng.uniform(0.2, 1.3, n_g)
+    phi = rng.uniform(-3.0, 3.0, n_g)
+    theta_obs = theta + rng.normal(0, 0.15, n_g)
+    phi_obs = phi + rng.normal(0, 0.15, n_g)
+    mask = lab >= 0
+    base6 = an.ti_stiffness_6(**an.ICE_MATERIAL)
+    K = 917.0 * 1500.0 ** 2
+    fl = np.zeros((6, 6))
+    fl[:3, :3] = K
+    Cbg = {k: np.full(lab.shape, fl[int(k[1]) - 1, int(k[2]) - 1]) for k in af.KEYS21}
+    h = p["h"]
+    dt = 0.4 * h / (np.sqrt(3.0) * 4100.0)
+    nt = 60
+    wav = sources_hann(nt, dt)
+    pts = [tuple(q) for q, _ in p["src_pts"]]
+    w = 1.0 / len(pts)
+    src_pts = [[(q, w) for q in pts]]
+    recs = [(pts, [w] * len(pts))]
+
+    def maps(th, ph):
+        cm = np.zeros(lab.shape)
+        am = np.zeros(lab.shape)
+        cm[mask] = th[lab[mask]]
+        am[mask] = ph[lab[mask]]
+        return cm, am
+
+    co, ao = maps(theta_obs, phi_obs)
+    Cobs, rho = af.build_maps(co, ao, mask, base6, Cbg, 917.0, 917.0)
+    dobs, _ = e3._grad_forward(Cobs, rho, h, dt, nt, None, wav, None, src_pts=src_pts[0],
+                               rec_groups=recs)
+    cm, am = maps(theta, phi)
+    J, g_t, g_p = af.misfit_and_gradient_axes(cm, am, mask, base6, Cbg, 917.0, 917.0, h, dt, nt,
+                                              src_pts, wav, recs, dobs[None])
+    gt = np.array([g_t[lab == g].sum() for g in range(n_g)])
+    gp = np.array([g_p[lab == g].sum() for g in range(n_g)])
+    np.savez_compressed(os.path.join(HERE, "adjoint_compat.npz"), lab=lab.astype(np.int16),
+                        theta=theta, phi=phi, h=h, dt=dt, nt=nt, wavelet=wav,
+                        pts=np.array(pts), dobs=dobs, J=J, g_theta=gt, g_phi=gp)
+
+
+def sources_hann(nt, dt):
+    from ringfwi import sources
+    return sources.hann_tone_burst(nt, dt, 2.0e6, n_cycles=2)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,157 @@
+"""The hand-written adjoint (GPU): gradients of trace misfits against central
+finite differences (stiffness table, per-grain c-axis angles at h = 1e-3 rad,
+fabric parameters) and against the reference's own gradient
+(vendor/ringfwi axisfield/elastic3d) in the matched order-2 configuration."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import make_small
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _problem(p, dtype="float64", K=7, record="vz", damped=True, mask=None, coeffs=None):
+    from pefdtd.adjoint import Problem
+    return Problem(p["mats"], p["rho_t"], p["h"], p["dt"], p["coeffs"] if coeffs is None else coeffs,
+                   p["src_pts"], p["rec_groups"], p["wavelet"], record=record,
+                   sponge_width=p["sponge"], damp_mask=mask, damped_record=damped, dtype=dtype,
+                   checkpoint_every=K)
+
+
+def _loss(prob, c21, dobs):
+    tr = prob.traces(c21)
+    return 0.5 * ((tr - dobs) ** 2).sum()
+
+
+def _c21_of(p):
+    from pefdtd.materials import c36_to_c21
+    from pefdtd.fdtd import _material_tables64
+    Ct, _ = _material_tables64(p["axes"], 1500.0, 300.0)
+    return c36_to_c21(Ct)
+
+
+@pytest.mark.parametrize("record,damped,masked", [("vz", True, False), ("pressure", False, True),
+                                                  ("pressure", True, False)])
+def test_table_gradient_vs_central_fd(record, damped, masked):
+    import torch
+    from pefdtd import damping
+    p = make_small(nt=70, shape=(18, 22, 24), n_grains=5, sponge=3, seed=21)
+    mask = damping.fluid_damp_mask(p["lab"], 0.05) if masked else None
+    prob = _problem(p, record=record, damped=damped, mask=mask, K=9)
+    c0 = torch.tensor(_c21_of(p))
+    with torch.no_grad():
+        dobs = prob.traces(c0 * 1.01) + 1e-3 * float(np.abs(prob.traces(c0).numpy()).max())
+    c = c0.clone().requires_grad_(True)
+    J = _loss(prob, c, dobs)
+    J.backward()
+    g = c.grad.numpy()
+    rng = np.random.default_rng(0)
+    d = torch.tensor(rng.standard_normal(c0.shape)) * c0.abs().mean()
+    def fd(eps):
+        with torch.no_grad():
+            return float((_loss(prob, c0 + eps * d, dobs) - _loss(prob, c0 - eps * d, dobs)) / (2 * eps))
+    # Richardson-extrapolated central difference (truncation O(eps^4))
+    f1, f2 = fd(2e-5), fd(1e-5)
+    fr = (4 * f2 - f1) / 3
+    ad = float((g * d.numpy()).sum())
+    assert abs(ad - fr) <= 1e-7 * abs(fr), (ad, f1, f2, fr)
+
+
+def test_grain_angle_gradient_vs_central_fd_1e3():
+    """20 random grains at h = 1e-3 rad, relative error <= 1e-3 (FP64 run);
+    the FP32 run of the same adjoint is reported against it."""
+    import torch
+    from pefdtd.adjoint import angles_from_axes, ice_table21
+    p = make_small(nt=90, shape=(20, 28, 28), n_grains=24, sponge=3, seed=8)
+    th0, ph0 = angles_from_axes(p["axes"])
+    prob = _problem(p, K=13)
+    with torch.no_grad():
+        dobs = prob.traces(ice_table21(torch.tensor(th0 + 0.05), torch.tensor(ph0 - 0.04)))
+    th = torch.tensor(th0, requires_grad=True)
+    ph = torch.tensor(ph0, requires_grad=True)
+    J = _loss(prob, ice_table21(th, ph), dobs)
+    J.backward()
+    gt, gp = th.grad.numpy(), ph.grad.numpy()
+    rng = np.random.default_rng(1)
+    grains = rng.choice(len(th0), size=20, replace=False)
+    h = 1e-3
+    errs = []
+    for g in grains:
+        for which in ("t", "p"):
+            tp, tm = th0.copy(), th0.copy()
+            pp, pm = ph0.copy(), ph0.copy()
+            if which == "t":
+                tp[g] += h
+                tm[g] -= h
+            else:
+                pp[g] += h
+                pm[g] -= h
+            with torch.no_grad():
+                fd = (_loss(prob, ice_table21(torch.tensor(tp), torch.tensor(pp)), dobs)
+                      - _loss(prob, ice_table21(torch.tensor(tm), torch.tensor(pm)), dobs)) / (2 * h)
+            ad = gt[g] if which == "t" else gp[g]
+            scale = max(abs(float(fd)), 1e-3 * np.abs(np.concatenate([gt, gp])).max())
+            errs.append(abs(ad - float(fd)) / scale)
+    assert max(errs) <= 1e-3, max(errs)
+    # FP32 kernels against the FP64 gradient
+    prob32 = _problem(p, dtype="float32", K=13)
+    th32 = torch.tensor(th0, requires_grad=True)
+    ph32 = torch.tensor(ph0, requires_grad=True)
+    _loss(prob32, ice_table21(th32, ph32), dobs).backward()
+    g64 = np.concatenate([gt, gp])
+    g32 = np.concatenate([th32.grad.numpy(), ph32.grad.numpy()])
+    assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)
+
+
+def test_fabric_parameter_gradient_vs_fd():
+    import torch
+    from pefdtd.adjoint import fabric_axes, ice_table21, theta_phi_torch
+    p = make_small(nt=60, shape=(18, 24, 24), n_grains=10, sponge=3, seed=4)
+    base = torch.tensor(p["axes"])
+    prob = _problem(p, K=11)
+
+    def table(params):
+        th, ph = theta_phi_torch(fabric_axes(params, base))
+        return ice_table21(th, ph)
+    with torch.no_grad():
+        dobs = prob.traces(table(torch.tensor([0.3, 0.2, 0.5])))
+    x0 = np.array([0.1, -0.3, 0.1])
+    x = torch.tensor(x0, requires_grad=True)
+    _loss(prob, table(x), dobs).backward()
+    g = x.grad.numpy()
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = 1e-4
+        with torch.no_grad():
+            fd = (_loss(prob, table(torch.tensor(x0 + e)), dobs)
+                  - _loss(prob, table(torch.tensor(x0 - e)), dobs)) / 2e-4
+        assert abs(g[k] - float(fd)) <= 1e-4 * max(abs(float(fd)), np.abs(g).max())
+
+
+def test_matches_reference_ringfwi_gradient():
+    """Order 2, no damping, pressure, uniform density: the configuration in
+    which the reference's ringfwi adjoint computes the same discrete
+    gradient (tests/golden/adjoint_compat.npz)."""
+    import torch
+    from pefdtd.adjoint import Problem, ice_table21
+    g = np.load(os.path.join(GOLD, "adjoint_compat.npz"))
+    lab = g["lab"].astype(np.int32)
+    n_mat = int(lab.max()) + 2
+    pts = [tuple(q) for q in g["pts"]]
+    w = 1.0 / len(pts)
+    prob = Problem((lab + 1).astype(np.uint16), np.full(n_mat, 917.0), float(g["h"]), float(g["dt"]),
+                   [1.0], [(q, w) for q in pts], [(pts, [w] * len(pts))], g["wavelet"],
+                   record="pressure", sponge_width=0, damped_record=False, dtype="float64",
+                   checkpoint_every=17)
+    th = torch.tensor(g["theta"], requires_grad=True)
+    ph = torch.tensor(g["phi"], requires_grad=True)
+    tr = prob.traces(ice_table21(th, ph, c_couplant=1500.0, rho_couplant=917.0))
+    J = 0.5 * ((tr - torch.tensor(g["dobs"])) ** 2).sum()
+    J.backward()
+    assert abs(float(J.detach()) - float(g["J"])) <= 1e-9 * float(g["J"])
+    ours = np.concatenate([th.grad.numpy(), ph.grad.numpy()])
+    ref = np.concatenate([g["g_theta"], g["g_phi"]])
+    assert np.linalg.norm(ours - ref) <= 1e-8 * np.linalg.norm(ref)
