@@ -195,9 +195,11 @@ int pe_solver_adjoint_step(PeSolver *s, const PeAdjoint *adj, int64_t n, const v
  * is ringfwi's elastic3d.forward_batch (vendor/ringfwi/elastic3d.py:474-632),
  * which stacks transmits on a leading array axis. Every solve keeps the
  * single-solve contract above (own grid size, medium, probe, wavelet, state
- * and traces); all share one dtype, the tiled kernels, nx a multiple of 4 and
- * 16-byte aligned state buffers. Each step is one stress and one velocity
- * launch covering every solve; chunks of steps replay as CUDA graphs. */
+ * and traces); all share one dtype and the tiled kernels. Each step is one
+ * stress and one velocity launch covering every solve with nx a multiple of
+ * 4 (state buffers 16-byte aligned), plus one launch pair per solve whose
+ * rows are not whole 16-byte units (the cp.async kernels); chunks of steps
+ * replay as CUDA graphs. */
 typedef struct PeBatch PeBatch;
 
 int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const PeProbe *probes,

@@ -902,6 +902,7 @@ struct PeBatch {
     bool uploaded = false;
     cudaGraphExec_t gexec = nullptr;
     long long launches = 0;
+    long long graph_launches = 0;   // kernels in one captured chunk
 
     ~PeBatch()
     {
@@ -932,6 +933,7 @@ int batch_layout(PeBatch *B)
         const int zc = (c.nz + nch - 1) / nch;
         B->solves[s]->zc_s = zc;
         B->solves[s]->zc_v = zc;
+        if (!B->solves[s]->tma_capable) continue;   // launched on its own
         const int nzc = (c.nz + zc - 1) / zc;
         for (int bz = 0; bz < nzc; ++bz) {
             for (int by = 0; by < (c.ny + pe::TS_OY - 1) / pe::TS_OY; ++by)
@@ -990,7 +992,8 @@ int batch_upload(PeBatch *B, const PeState *states, void *const *traces)
         PeSolver *S = B->solves[s];
         int rc = ensure_maps(S, &states[s]);
         if (rc) return rc;
-        if (!S->tma) return fail(PE_ERR_UNSUPPORTED, "batched solves need 16-byte aligned state buffers");
+        if (S->tma_capable && !S->tma)
+            return fail(PE_ERR_UNSUPPORTED, "batched solves need 16-byte aligned state buffers");
         descs[s] = make_args<T>(S, &states[s], 0);
         descs[s].step = B->step;
         descs[s].status = B->status;
@@ -1016,11 +1019,25 @@ int batch_chunk(PeBatch *B, int len)
 {
     const dim3 block(pe::TB_X, pe::TB_Y, 1);
     for (int k = 0; k < len; ++k) {
-        pe::k_stress_tma_batch<T><<<B->grid_s, block, B->smem_s, B->stream>>>(
-            (const pe::StepArgs<T> *)B->descs, B->maps_s, B->nmats, B->items_s, B->n_items_s, k);
-        pe::k_velocity_tma_batch<T><<<B->grid_v, block, B->smem_v, B->stream>>>(
-            (const pe::StepArgs<T> *)B->descs, B->maps_v, B->nmats, B->items_v, B->n_items_v, k);
-        B->launches += 2;
+        if (B->n_items_s > 0) {
+            pe::k_stress_tma_batch<T><<<B->grid_s, block, B->smem_s, B->stream>>>(
+                (const pe::StepArgs<T> *)B->descs, B->maps_s, B->nmats, B->items_s, B->n_items_s, k);
+            pe::k_velocity_tma_batch<T><<<B->grid_v, block, B->smem_v, B->stream>>>(
+                (const pe::StepArgs<T> *)B->descs, B->maps_v, B->nmats, B->items_v, B->n_items_v, k);
+            B->launches += 2;
+        }
+        // solves whose rows are not whole 16-byte units run the cp.async
+        // kernels, one launch pair each, on the same stream and step counter
+        for (int s = 0; s < (int)B->solves.size(); ++s) {
+            PeSolver *S = B->solves[s];
+            if (S->tma_capable) continue;
+            pe::StepArgs<T> A = make_args<T>(S, &B->states[s], k);
+            A.step = B->step;
+            A.status = B->status;
+            launch_stress<T>(S, A, B->stream);
+            launch_velocity<T>(S, A, B->stream);
+            B->launches += 2;
+        }
     }
     for (int s = 0; s < (int)B->solves.size(); ++s) {
         PeSolver *S = B->solves[s];
@@ -1057,15 +1074,14 @@ int batch_run_t(PeBatch *B, const PeState *states, void *const *traces, int64_t 
                 cudaError_t ce = cudaStreamEndCapture(B->stream, &g);
                 if (rc) return rc;
                 if (ce != cudaSuccess) return fail(PE_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+                B->graph_launches = B->launches - before;
                 B->launches = before;
                 ce = cudaGraphInstantiate(&B->gexec, g, 0);
                 cudaGraphDestroy(g);
                 if (ce != cudaSuccess) return fail(PE_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ce));
             }
             PE_CUDA(cudaGraphLaunch(B->gexec, B->stream));
-            int nred = 0;
-            for (PeSolver *S : B->solves) nred += S->n_groups > 0;
-            B->launches += 2LL * len + nred + 1;
+            B->launches += B->graph_launches;
         } else if ((rc = batch_chunk<T>(B, len))) {
             return rc;
         }
@@ -1096,10 +1112,6 @@ int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const Pe
         int rc = pe_solver_create(&cfgs[s], &media[s], &probes[s], &S);
         if (rc) return fail(rc, "solve " + std::to_string(s) + ": " + g_err);
         B->solves.push_back(S);
-        if (!S->tma_capable)
-            return fail(PE_ERR_UNSUPPORTED, "solve " + std::to_string(s) +
-                                                ": batched solves need nx a multiple of 4");
-        B->chunk = std::max(B->chunk, 1);
     }
     B->chunk = cfgs[0].chunk_steps > 0 ? cfgs[0].chunk_steps : 200;
     int rc;

@@ -141,6 +141,203 @@ def orientation_tensor(axes):
     return w[o], V[:, o]
 
 
+def assign_shortlist(P, seeds, weights, k=12):
+    """Laguerre assignment through the k Euclidean-nearest seeds (the CPU
+    labeller of sim/core/specimen.py:339-351; exact while the weight spread
+    is modest). Returns int16 seed indices."""
+    from scipy.spatial import cKDTree
+    k = min(k, len(seeds))
+    _, idx = cKDTree(seeds).query(P, k=k, workers=-1)
+    idx = np.atleast_2d(idx.T).T
+    d2 = ((P[:, None, :] - seeds[idx]) ** 2).sum(-1) - weights[idx]
+    return idx[np.arange(len(P)), d2.argmin(1)].astype(np.int16)
+
+
+def adjacency(labels):
+    """Grain adjacency {label: set(neighbour labels)} over face neighbours."""
+    adj = {}
+    for ax in range(3):
+        a = np.take(labels, np.arange(labels.shape[ax] - 1), axis=ax)
+        b = np.take(labels, np.arange(1, labels.shape[ax]), axis=ax)
+        m = (a != b) & (a >= 0) & (b >= 0)
+        for u, v in np.unique(np.stack([a[m], b[m]], 1), axis=0):
+            adj.setdefault(int(u), set()).add(int(v))
+            adj.setdefault(int(v), set()).add(int(u))
+    return adj
+
+
+def renormalise_fabric(axes, target_a1, n_iter=60):
+    """Rescale every axis's angle from the dominant eigenvector until the
+    largest orientation-tensor eigenvalue is back at target_a1."""
+    w, V = orientation_tensor(axes)
+    if abs(w[0] - target_a1) < 1e-4:
+        return axes
+    e1 = V[:, 0]
+    sgn = np.sign(axes @ e1)
+    sgn[sgn == 0] = 1.0
+    a = axes * sgn[:, None]
+    cos = np.clip(a @ e1, -1.0, 1.0)
+    psi = np.arccos(cos)
+    perp = a - cos[:, None] * e1[None, :]
+    pn = np.linalg.norm(perp, axis=1, keepdims=True)
+    perp = np.divide(perp, np.maximum(pn, 1e-12), out=np.zeros_like(perp), where=pn > 1e-12)
+
+    def rebuild(k):
+        p2 = np.minimum(psi * k, np.pi / 2)
+        return np.cos(p2)[:, None] * e1[None, :] + np.sin(p2)[:, None] * perp
+
+    lo, hi = 0.0, 6.0
+    for _ in range(n_iter):
+        k = 0.5 * (lo + hi)
+        if orientation_tensor(rebuild(k))[0][0] > target_a1:
+            lo = k
+        else:
+            hi = k
+    out = rebuild(0.5 * (lo + hi))
+    return out / np.linalg.norm(out, axis=1, keepdims=True)
+
+
+class DiskSpecimen:
+    """Laguerre-polycrystal ice disk with a Watson c-axis fabric.
+
+    Same controls, random stream and results as the reference's
+    ``DiskSpecimen`` (sim/core/specimen.py:166-279): the seed count and
+    Laguerre weight scale are calibrated on Monte-Carlo points (12-nearest
+    shortlist) to the requested grain-size CV, the grid is then labelled with
+    the exact all-seeds power argmin (on the GPU when one is available, else
+    with the shortlist, as the reference falls back), empty cells are dropped,
+    c-axes are Watson-sampled and optionally smoothed toward neighbours.
+    """
+
+    def __init__(self, diameter_m=100e-3, thickness_m=35e-3, n_grains=400, size_cv=0.35,
+                 concentration=4.0, spatial_corr=0.0, fabric_axis=(0.0, 0.0, 1.0), seed=7):
+        self.diameter_m, self.thickness_m, self.n_grains = diameter_m, thickness_m, n_grains
+        self.size_cv, self.concentration, self.spatial_corr = size_cv, concentration, spatial_corr
+        self.fabric_axis, self.seed = tuple(fabric_axis), seed
+
+    @staticmethod
+    def _mc_points(R, thickness, n, rng):
+        p = rng.uniform(-1, 1, (int(n * 1.4), 3))
+        p = p[(p[:, 0] ** 2 + p[:, 1] ** 2) <= 1.0][:n]
+        p[:, :2] *= R
+        p[:, 2] *= thickness / 2
+        return p
+
+    def calibrate(self, rng):
+        R = self.diameter_m / 2
+        mc = self._mc_points(R, self.thickness_m, 400000, rng)
+        base = (R / self.n_grains ** (1 / 3)) ** 2
+        sigma = np.sqrt(np.log(1 + self.size_cv ** 2))
+        n_seed = self.n_grains
+        for outer in range(4):
+            seeds = seed_points(R, self.thickness_m, n_seed, rng)
+            radii = rng.lognormal(-0.5 * sigma ** 2, sigma, n_seed)
+            wshape = base * (radii ** 2 - 1.0)
+            lo, hi, scale = 0.0, 8.0, 0.0
+            for _ in range(20):
+                trial = 0.5 * (lo + hi)
+                cnt = np.bincount(assign_shortlist(mc, seeds, trial * wshape), minlength=n_seed).astype(float)
+                live = cnt[cnt > 0]
+                cv = (live ** (1 / 3)).std() / (live ** (1 / 3)).mean()
+                if cv < self.size_cv:
+                    lo = trial
+                else:
+                    hi = trial
+                scale = trial
+            n_live = int((np.bincount(assign_shortlist(mc, seeds, scale * wshape),
+                                      minlength=n_seed) > 0).sum())
+            if n_live >= self.n_grains or outer == 3:
+                break
+            n_seed = int(np.ceil(n_seed * self.n_grains / max(n_live, 1)))
+        return seeds, scale * wshape, n_seed
+
+    def build(self, h, use_gpu=None):
+        rng = np.random.default_rng(self.seed)
+        R = self.diameter_m / 2
+        nx = int(np.ceil(self.diameter_m / h))
+        nz = int(np.ceil(self.thickness_m / h))
+        seeds, weights, n_seed = self.calibrate(rng)
+        x = (np.arange(nx) - (nx - 1) / 2) * h
+        z = (np.arange(nz) - (nz - 1) / 2) * h
+        if use_gpu is None:
+            try:
+                import torch
+                use_gpu = torch.cuda.is_available()
+            except Exception:
+                use_gpu = False
+        if use_gpu:
+            raw = label_cylinder(x, x, z, R, seeds, weights).cpu().numpy().transpose(2, 1, 0)
+        else:
+            X, Y, Z = np.meshgrid(x, x, z, indexing="ij")
+            inside = (X ** 2 + Y ** 2) <= R ** 2
+            raw = np.full(X.shape, -1, np.int32)
+            P = np.stack([X[inside], Y[inside], Z[inside]], axis=1)
+            raw[inside] = assign_shortlist(P, seeds, weights).astype(np.int32)
+        inside = raw >= 0
+        keep = np.unique(raw[inside])
+        remap = np.full(len(seeds), -1, np.int32)
+        remap[keep] = np.arange(len(keep))
+        labels = np.full(raw.shape, -1, np.int16)
+        labels[inside] = remap[raw[inside]].astype(np.int16)
+        axes = sample_watson(len(keep), self.fabric_axis, self.concentration, rng)
+        adj = adjacency(labels)
+        if self.spatial_corr > 0:
+            target_a1 = orientation_tensor(axes)[0][0]
+            for _ in range(3):
+                nb = np.zeros_like(axes)
+                for g, ns in adj.items():
+                    if ns:
+                        v = axes[list(ns)]
+                        v = v * np.sign(v @ axes[g])[:, None]
+                        nb[g] = v.mean(axis=0)
+                    else:
+                        nb[g] = axes[g]
+                axes = (1 - self.spatial_corr) * axes + self.spatial_corr * nb
+                axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+            axes = renormalise_fabric(axes, target_a1)
+        return dict(labels=labels, axes=axes, seeds=seeds[keep], weights=weights[keep],
+                    adjacency=adj, h=h, inside=inside, shape=labels.shape, n_seed=n_seed)
+
+
+def rotated_grid_single_raster(build, h, sponge, rot_deg, use_gpu=None):
+    """Solver grid of the specimen rotated by -rot_deg about z, labelled by
+    evaluating the Laguerre tessellation at the solver points (seeds rotated
+    instead of the points; the reference's single_raster path,
+    sim/core/rotation_test.py:93-127). Returns (lab, nd, m, axes_rot)."""
+    labels, h_spec = build["labels"], build["h"]
+    nx_s, _, nz_s = labels.shape
+    D = nx_s * h_spec
+    nd = int(round(D / h))
+    ndz = int(round(nz_s * h_spec / h))
+    a = np.radians(rot_deg)
+    ca, sa = np.cos(a), np.sin(a)
+    u = (np.arange(nd) + 0.5) * h - D / 2.0
+    Rd = 0.5 * D
+    zc = (np.arange(ndz) - (ndz - 1) / 2) * h
+    Rm = np.array([[ca, -sa, 0.0], [sa, ca, 0.0], [0.0, 0.0, 1.0]])
+    sd = np.asarray(build["seeds"], float) @ Rm
+    wts = np.asarray(build["weights"], float)
+    if use_gpu is None:
+        try:
+            import torch
+            use_gpu = torch.cuda.is_available()
+        except Exception:
+            use_gpu = False
+    if use_gpu:
+        core = label_cylinder(u, u, zc, Rd, sd, wts).cpu().numpy()
+    else:
+        X3, Y3, Z3 = np.meshgrid(u, u, zc, indexing="ij")
+        ins = (X3 ** 2 + Y3 ** 2) <= Rd ** 2
+        raw = np.full(X3.shape, -1, np.int32)
+        raw[ins] = assign_shortlist(np.stack([X3[ins], Y3[ins], Z3[ins]], 1), sd, wts).astype(np.int32)
+        core = raw.transpose(2, 1, 0)
+    m = sponge + 3
+    nz, nx = ndz + 2 * m, nd + 2 * m
+    lab = np.full((nz, nx, nx), -1, np.int32)
+    lab[m:m + ndz, m:m + nd, m:m + nd] = core
+    return lab, nd, m, np.asarray(build["axes"], float) @ Rm
+
+
 def build_grid(labels_xyz, h_spec, h, sponge):
     """Nearest-sample a specimen label volume (x, y, z) at spacing h_spec onto
     the solver grid at spacing h and pad by sponge + 3 fluid cells; returns

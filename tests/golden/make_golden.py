@@ -113,6 +113,15 @@ def main():
                         seeds=b["seeds"], weights=b["weights"], h=b["h"], grid_lab=g_lab,
                         rot17=r_lab17, rot17_axes=r_ax17, rot90=r_lab90, rot90_axes=r_ax90,
                         watson=wat, watson_girdle=wat_g, seed_pts=seeds)
+    # single-raster rotation (seeds rotated, shortlist labeller) and a
+    # neighbour-smoothed fabric
+    s_lab, _, _, s_ax = RT.rotated_grid(b, 0.4e-3, 4, 33, single_raster=True)
+    sp2 = spm.DiskSpecimen(diameter_m=0.010, thickness_m=0.005, n_grains=30, size_cv=0.5,
+                           concentration=-2.0, spatial_corr=0.4, fabric_axis=(0, 1, 1), seed=11)
+    b2 = sp2.build(0.5e-3)
+    np.savez_compressed(os.path.join(HERE, "specimen2.npz"), rot33_single=s_lab, rot33_axes=s_ax,
+                        labels=b2["labels"], axes=b2["axes"], seeds=b2["seeds"],
+                        weights=b2["weights"])
 
     # ---- forward traces on a small seeded disk
     sys.path.insert(0, os.path.dirname(HERE))

@@ -1,6 +1,6 @@
 """Batched solves (GPU): each solve of a mixed-size batch is bit-identical to
 its own single solve and to the oracle; the autotuner leaves results
-unchanged; the batch refuses what it cannot run."""
+unchanged; solves the TMA kernels cannot take run in the same graph."""
 import numpy as np
 import pytest
 
@@ -69,6 +69,44 @@ def test_forward_batch_convenience_and_refusals():
     for p, tr in zip(probs, out):
         ref = O.run_oracle(oracle_prob(p, record=p["record"], damped_record=True), fma_mode=1)
         assert np.array_equal(tr, ref)
-    bad = make_small(nt=20, shape=(16, 20, 30), n_grains=4, sponge=2)   # nx % 4 != 0
-    with pytest.raises(Exception, match="multiple of 4"):
-        batch.BatchSolver([batch.spec_from_problem(bad)])
+    with pytest.raises(ValueError, match="empty"):
+        batch.BatchSolver([])
+    with pytest.raises(Exception, match="wavelet shorter"):
+        b = batch.BatchSolver([batch.spec_from_problem(probs[0])])
+        try:
+            b.run(0, probs[0]["nt"] + 1)
+        finally:
+            b.close()
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_mixed_batch_with_unaligned_rows(dtype):
+    """Solves with nx % 4 != 0 (the cp.async kernels) ride in the same graph
+    as TMA-fed solves; every one stays bit-identical to the oracle."""
+    from pefdtd import batch
+    probs = [make_small(nt=70, shape=(16, 20, 30), n_grains=4, sponge=2, seed=3),
+             make_small(nt=70, shape=(20, 28, 32), n_grains=6, sponge=3, seed=4),
+             make_small(nt=70, shape=(18, 22, 27), n_grains=5, sponge=3, seed=5)]
+    probs[2]["record"] = "pressure"
+    b = batch.BatchSolver([batch.spec_from_problem(p) for p in probs], dtype=dtype, z_chunk=9,
+                          chunk_steps=30)
+    try:
+        b.run(0, 70)
+        got = b.traces_numpy(70)
+        # 70 steps: two graph chunks and a 10-step tail; 2 + 2*2 kernels per step
+        assert b.launch_count() == 70 * 6 + 3 * 3 + 3 + 1
+    finally:
+        b.close()
+    for p, tr in zip(probs, got):
+        npdt = np.dtype(dtype)
+        ref = O.run_oracle(oracle_prob(p, record=p["record"], damped_record=True, dtype=npdt),
+                           dtype=npdt, fma_mode=1)
+        assert np.array_equal(tr, ref)
+
+
+def test_batch_of_only_unaligned_rows():
+    from pefdtd import batch
+    probs = [make_small(nt=40, shape=(15, 19, 23), n_grains=4, sponge=2, seed=9)]
+    out = batch.forward_batch(probs, autotune=False)
+    ref = O.run_oracle(oracle_prob(probs[0], record=probs[0]["record"], damped_record=True), fma_mode=1)
+    assert np.array_equal(out[0], ref)

@@ -86,6 +86,25 @@ def test_specimen_label_builders_bit_exact():
         assert np.array_equal(ax_r, g[f"rot{deg}_axes"])
 
 
+def test_disk_specimen_build_bit_exact():
+    """The restated DiskSpecimen (Laguerre calibration on the reference's
+    random stream, shortlist labeller as the reference falls back without a
+    GPU) gives the reference's labels, seeds, weights and c-axes."""
+    g, g2 = _g("specimen.npz"), _g("specimen2.npz")
+    sp = specimen.DiskSpecimen(diameter_m=0.012, thickness_m=0.006, n_grains=25, size_cv=0.35,
+                               concentration=3.0, spatial_corr=0.0, fabric_axis=(1, 0, 0), seed=7)
+    b = sp.build(0.5e-3, use_gpu=False)
+    for k in ("labels", "axes", "seeds", "weights"):
+        assert np.array_equal(b[k], g[k]), k
+    lab, nd, m, ax = specimen.rotated_grid_single_raster(b, 0.4e-3, 4, 33, use_gpu=False)
+    assert np.array_equal(lab, g2["rot33_single"]) and np.array_equal(ax, g2["rot33_axes"])
+    sp2 = specimen.DiskSpecimen(diameter_m=0.010, thickness_m=0.005, n_grains=30, size_cv=0.5,
+                                concentration=-2.0, spatial_corr=0.4, fabric_axis=(0, 1, 1), seed=11)
+    b2 = sp2.build(0.5e-3, use_gpu=False)
+    for k in ("labels", "axes", "seeds", "weights"):
+        assert np.array_equal(b2[k], g2[k]), k
+
+
 def test_sampling_matches_reference_streams():
     g = _g("specimen.npz")
     rng = np.random.default_rng(3)
