@@ -262,15 +262,14 @@ def _coeffs_or_default(coeffs, order):
     return np.asarray(coeffs, float).reshape(-1)
 
 
-def forward_fused_labels(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, order=8,
-                         coeffs=None, sponge_width=0, sponge_strength=0.09, damp_mask=None,
-                         c_couplant=1500.0, rho_couplant=300.0, record="pressure", slab=32,
-                         stress_smem=False, progress=None, mat_tables=None, *,
-                         dtype="float32", damped_record=False, device=None, chunk_steps=0,
-                         tile=(0, 0), z_chunk=0, variant="tiled", return_solve=False):
-    """Label-indexed solve; returns the (nt, n_rec) traces as float32 (float64
-    when dtype="float64"). ``slab`` and ``stress_smem`` are accepted for
-    signature compatibility; the kernels march z without slabs."""
+def label_solve_spec(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coeffs=None,
+                     sponge_width=0, sponge_strength=0.09, damp_mask=None, c_couplant=1500.0,
+                     rho_couplant=300.0, record="pressure", mat_tables=None, *, dtype="float32",
+                     damped_record=False):
+    """Host half of :func:`forward_fused_labels`: checks its arguments as the
+    reference does (:1638-1722) and returns the solve description
+    (keyword arguments of :func:`c_solve_structs` plus ``wavelet``) that
+    :class:`DeviceSolve` and :class:`pefdtd.batch.BatchSolver` take."""
     coeffs = _coeffs_or_default(coeffs, order)
     if len(coeffs) > 4:
         raise ValueError(
@@ -313,11 +312,30 @@ def forward_fused_labels(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, ord
                     f"{int(bad[0])}): the deferred-damping scheme records pre-damp stress there "
                     f"and would silently diverge from the dense path. Move the footprint out of "
                     f"the sponge/fluid-damped region (or pass damped_record=True).")
-    solve = DeviceSolve(mats, Ct, rho_t, h, dt, coeffs, s_idx, s_w, r_off, r_idx, r_w,
-                        record=record, damped_record=damped_record, sponge=sponge,
-                        damp_volume=dm, dtype=dtype, device=device, chunk_steps=chunk_steps,
-                        tile=tile, z_chunk=z_chunk, variant=variant)
-    solve.set_wavelet(np.asarray(wavelet, float)[:nt])
+    return dict(mats=mats, Ct=Ct, rho_t=rho_t, h=h, dt=dt, coeffs=coeffs, src_idx=s_idx,
+                src_w=s_w, rec_off=r_off, rec_idx=r_idx, rec_w=r_w, record=record,
+                damped_record=damped_record, sponge=sponge, damp_volume=dm,
+                wavelet=np.asarray(wavelet, float)[:int(nt)])
+
+
+def forward_fused_labels(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, order=8,
+                         coeffs=None, sponge_width=0, sponge_strength=0.09, damp_mask=None,
+                         c_couplant=1500.0, rho_couplant=300.0, record="pressure", slab=32,
+                         stress_smem=False, progress=None, mat_tables=None, *,
+                         dtype="float32", damped_record=False, device=None, chunk_steps=0,
+                         tile=(0, 0), z_chunk=0, variant="tiled", return_solve=False):
+    """Label-indexed solve; returns the (nt, n_rec) traces as float32 (float64
+    when dtype="float64"). ``slab`` and ``stress_smem`` are accepted for
+    signature compatibility; the kernels march z without slabs."""
+    sp = label_solve_spec(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, order, coeffs,
+                          sponge_width, sponge_strength, damp_mask, c_couplant, rho_couplant,
+                          record, mat_tables, dtype=dtype, damped_record=damped_record)
+    wav = sp.pop("wavelet")
+    solve = DeviceSolve(sp.pop("mats"), sp.pop("Ct"), sp.pop("rho_t"), sp.pop("h"), sp.pop("dt"),
+                        sp.pop("coeffs"), sp.pop("src_idx"), sp.pop("src_w"), sp.pop("rec_off"),
+                        sp.pop("rec_idx"), sp.pop("rec_w"), **sp, dtype=dtype, device=device,
+                        chunk_steps=chunk_steps, tile=tile, z_chunk=z_chunk, variant=variant)
+    solve.set_wavelet(wav)
     try:
         _run_with_progress(solve, int(nt), progress)
         out = solve.traces_numpy(int(nt))

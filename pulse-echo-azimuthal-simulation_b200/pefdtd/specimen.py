@@ -251,7 +251,11 @@ class DiskSpecimen:
             n_seed = int(np.ceil(n_seed * self.n_grains / max(n_live, 1)))
         return seeds, scale * wshape, n_seed
 
-    def build(self, h, use_gpu=None):
+    def build(self, h, use_gpu=None, labeller=None):
+        """Label volume (x, y, z), c-axes, seeds and weights at spacing h.
+        ``labeller``: "gpu" (exact, pe_label_cylinder), "exact" (the same
+        argmin in NumPy) or "shortlist" (the reference's CPU fallback);
+        default "gpu" when a CUDA device is present, else "shortlist"."""
         rng = np.random.default_rng(self.seed)
         R = self.diameter_m / 2
         nx = int(np.ceil(self.diameter_m / h))
@@ -259,20 +263,7 @@ class DiskSpecimen:
         seeds, weights, n_seed = self.calibrate(rng)
         x = (np.arange(nx) - (nx - 1) / 2) * h
         z = (np.arange(nz) - (nz - 1) / 2) * h
-        if use_gpu is None:
-            try:
-                import torch
-                use_gpu = torch.cuda.is_available()
-            except Exception:
-                use_gpu = False
-        if use_gpu:
-            raw = label_cylinder(x, x, z, R, seeds, weights).cpu().numpy().transpose(2, 1, 0)
-        else:
-            X, Y, Z = np.meshgrid(x, x, z, indexing="ij")
-            inside = (X ** 2 + Y ** 2) <= R ** 2
-            raw = np.full(X.shape, -1, np.int32)
-            P = np.stack([X[inside], Y[inside], Z[inside]], axis=1)
-            raw[inside] = assign_shortlist(P, seeds, weights).astype(np.int32)
+        raw = _label_xyz(x, z, R, seeds, weights, pick_labeller(use_gpu, labeller))
         inside = raw >= 0
         keep = np.unique(raw[inside])
         remap = np.full(len(seeds), -1, np.int32)
@@ -299,7 +290,36 @@ class DiskSpecimen:
                     adjacency=adj, h=h, inside=inside, shape=labels.shape, n_seed=n_seed)
 
 
-def rotated_grid_single_raster(build, h, sponge, rot_deg, use_gpu=None):
+def pick_labeller(use_gpu=None, labeller=None):
+    if labeller is not None:
+        if labeller not in ("gpu", "exact", "shortlist"):
+            raise ValueError(f"labeller must be 'gpu', 'exact' or 'shortlist', got {labeller!r}")
+        return labeller
+    if use_gpu is None:
+        try:
+            import torch
+            use_gpu = torch.cuda.is_available()
+        except Exception:
+            use_gpu = False
+    return "gpu" if use_gpu else "shortlist"
+
+
+def _label_xyz(x, z, R, seeds, weights, how):
+    """(nx, nx, nz) int32 power-diagram labels of the cylinder r <= R on the
+    square grid x by x by z; -1 outside."""
+    if how == "gpu":
+        return label_cylinder(x, x, z, R, seeds, weights).cpu().numpy().transpose(2, 1, 0)
+    if how == "exact":
+        return label_cylinder_numpy(x, x, z, R, seeds, weights).transpose(2, 1, 0)
+    X, Y, Z = np.meshgrid(x, x, z, indexing="ij")
+    inside = (X ** 2 + Y ** 2) <= R ** 2
+    raw = np.full(X.shape, -1, np.int32)
+    raw[inside] = assign_shortlist(np.stack([X[inside], Y[inside], Z[inside]], 1), seeds,
+                                   weights).astype(np.int32)
+    return raw
+
+
+def rotated_grid_single_raster(build, h, sponge, rot_deg, use_gpu=None, labeller=None):
     """Solver grid of the specimen rotated by -rot_deg about z, labelled by
     evaluating the Laguerre tessellation at the solver points (seeds rotated
     instead of the points; the reference's single_raster path,
@@ -317,20 +337,7 @@ def rotated_grid_single_raster(build, h, sponge, rot_deg, use_gpu=None):
     Rm = np.array([[ca, -sa, 0.0], [sa, ca, 0.0], [0.0, 0.0, 1.0]])
     sd = np.asarray(build["seeds"], float) @ Rm
     wts = np.asarray(build["weights"], float)
-    if use_gpu is None:
-        try:
-            import torch
-            use_gpu = torch.cuda.is_available()
-        except Exception:
-            use_gpu = False
-    if use_gpu:
-        core = label_cylinder(u, u, zc, Rd, sd, wts).cpu().numpy()
-    else:
-        X3, Y3, Z3 = np.meshgrid(u, u, zc, indexing="ij")
-        ins = (X3 ** 2 + Y3 ** 2) <= Rd ** 2
-        raw = np.full(X3.shape, -1, np.int32)
-        raw[ins] = assign_shortlist(np.stack([X3[ins], Y3[ins], Z3[ins]], 1), sd, wts).astype(np.int32)
-        core = raw.transpose(2, 1, 0)
+    core = _label_xyz(u, zc, Rd, sd, wts, pick_labeller(use_gpu, labeller)).transpose(2, 1, 0)
     m = sponge + 3
     nz, nx = ndz + 2 * m, nd + 2 * m
     lab = np.full((nz, nx, nx), -1, np.int32)

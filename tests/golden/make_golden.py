@@ -15,6 +15,8 @@ run time):
   forward_small.npz  fdtd.forward traces (FP64 on CPU, and FP32 through a
                      NumPy stand-in for CuPy) for a small seeded disk, both
                      records, with the inputs that produced them
+  sweep_protocol.npz the sweep engine's per-azimuth solver arguments and
+                     az{ddd}.npz files on a coarse disk; azimuth orders
 """
 from __future__ import annotations
 
@@ -148,7 +150,83 @@ def main():
         res[f"{record}_f32"] = tr32
     np.savez_compressed(os.path.join(HERE, "forward_small.npz"), **res)
     adjoint_compat()
+    sweep_protocol()
     print("golden fixtures written to", HERE)
+
+
+SWEEP_CFG = dict(f0_mhz=0.5, ppw=6.0, az_start=0, az_stop=360, az_step=45, diameter_mm=80.0,
+                 thickness_mm=10.0, n_grains=12, sponge=10, seed=5)
+
+
+def sweep_protocol():
+    """The reference sweep engine (sim/pipeline/sweep_runner.py) run on a
+    coarse 80 mm disk with a NumPy stand-in for CuPy (so its exact all-seeds
+    labeller runs) and forward_fused_labels replaced by a recorder that
+    returns tests/helpers.synthetic_echo: every solver argument it passes
+    per azimuth, and the az{ddd}.npz files it writes."""
+    import hashlib
+    import shutil
+    import tempfile
+    sys.path.insert(0, os.path.join(REF, "sim", "pipeline"))
+    sys.path.insert(0, os.path.dirname(HERE))
+    from helpers import synthetic_echo
+    cp = _numpy_as_cupy()
+    cp.cuda.runtime.getDeviceProperties = lambda i: {"name": b"numpy"}
+    sys.modules["cupy"] = cp
+    import sweep_runner as SR
+    import fdtd as F
+    calls = {}
+
+    def recorder(lab, axes, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coeffs=None,
+                 sponge_width=0, damp_mask=None, progress=None, **kw):
+        az = len(calls)
+        calls[az] = dict(lab=lab, axes=axes, h=h, dt=dt, nt=nt, src=src_pts, wav=wavelet,
+                         rec=rec_groups, order=order, coeffs=coeffs, sponge=sponge_width,
+                         dm=damp_mask)
+        if progress is not None:
+            progress(0.0)
+        return synthetic_echo(nt, dt, 0.5e6)[:, None]
+    orig = F.forward_fused_labels
+    F.forward_fused_labels = recorder
+    tmp = tempfile.mkdtemp()
+    try:
+        SR.SWEEPS = tmp
+        SR.create("fx", **SWEEP_CFG)
+        cfg = SR.load("fx")
+        order = SR.azimuths(cfg)
+        SR.run(cfg)
+        res = dict(order=np.array(order))
+        sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
+        for i, az in enumerate(order):
+            c = calls[i]
+            with np.load(os.path.join(tmp, "fx", f"az{az:03d}.npz")) as z:
+                for k in z.files:
+                    res[f"{az}_file_{k}"] = z[k]
+            res[f"{az}_lab_shape"] = np.array(c["lab"].shape)
+            res[f"{az}_lab_sha"] = sha(np.asarray(c["lab"], np.int32))
+            res[f"{az}_dm_sha"] = sha(np.asarray(c["dm"], np.float32))
+            res[f"{az}_wav_sha"] = sha(np.asarray(c["wav"], np.float64))
+            res[f"{az}_axes"] = np.asarray(c["axes"])
+            res[f"{az}_dt"] = c["dt"]
+            res[f"{az}_nt"] = c["nt"]
+            res[f"{az}_src"] = np.array([p for p, _ in c["src"]])
+            res[f"{az}_w"] = c["src"][0][1]
+            res[f"{az}_coeffs"] = np.asarray(c["coeffs"])
+        with open(os.path.join(tmp, "fx", "status.json")) as f:
+            res["final_phase"] = json.load(f)["phase"]
+        orders = {}
+        for n in range(0, 70):
+            orders[f"bitrev_{n}"] = np.array(SR._bit_reversed_order(n), np.int64)
+        for start, stop, step, mode in ((0, 360, 1, "progressive"), (10, 350, 7, "progressive"),
+                                        (0, 180, 4, "progressive"), (0, 360, 5, "sequential")):
+            c2 = dict(az_start=start, az_stop=stop, az_step=step, sweep_order=mode)
+            orders[f"az_{start}_{stop}_{step}_{mode}"] = np.array(SR.azimuths(c2), np.int64)
+        res.update(orders)
+        np.savez_compressed(os.path.join(HERE, "sweep_protocol.npz"), **res)
+    finally:
+        F.forward_fused_labels = orig
+        del sys.modules["cupy"]
+        shutil.rmtree(tmp)
 
 
 def adjoint_compat():

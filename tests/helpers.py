@@ -37,3 +37,13 @@ def rel_l2(a, b):
     a = np.asarray(a, float)
     b = np.asarray(b, float)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def synthetic_echo(nt, dt, f0):
+    """A deterministic stand-in trace for sweep-protocol tests: a Gaussian
+    burst at the 2 x 100 mm first-echo time plus a weak later coda."""
+    t = np.arange(int(nt)) * float(dt)
+    t1 = 0.200 / 3850.0
+    burst = np.sin(2 * np.pi * f0 * (t - t1)) * np.exp(-((t - t1) * f0 / 1.5) ** 2)
+    coda = 0.05 * np.sin(2 * np.pi * 0.7 * f0 * t) * np.exp(-((t - 30e-6) / 8e-6) ** 2)
+    return (burst + coda).astype(np.float32)
