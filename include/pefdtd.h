@@ -198,8 +198,9 @@ int pe_solver_adjoint_step(PeSolver *s, const PeAdjoint *adj, int64_t n, const v
  * and traces); all share one dtype and the tiled kernels. Each step is one
  * stress and one velocity launch covering every solve with nx a multiple of
  * 4 (state buffers 16-byte aligned), plus one launch pair per solve whose
- * rows are not whole 16-byte units (the cp.async kernels); chunks of steps
- * replay as CUDA graphs. */
+ * rows are not whole 16-byte units (the cp.async kernels); when the batched
+ * kernels' shared memory cannot hold the largest table (FP64), every solve
+ * runs its own pair. Chunks of steps replay as CUDA graphs. */
 typedef struct PeBatch PeBatch;
 
 int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const PeProbe *probes,

@@ -903,6 +903,7 @@ struct PeBatch {
     cudaGraphExec_t gexec = nullptr;
     long long launches = 0;
     long long graph_launches = 0;   // kernels in one captured chunk
+    bool tma_batch = true;          // the batched TMA kernels fit this batch
 
     ~PeBatch()
     {
@@ -920,6 +921,9 @@ struct PeBatch {
 
 namespace {
 
+// Whether solve S runs inside the batched TMA launches (else its own pair).
+bool batched(const PeBatch *B, const PeSolver *S) { return B->tma_batch && S->tma_capable; }
+
 template <typename T>
 int batch_layout(PeBatch *B)
 {
@@ -927,20 +931,12 @@ int batch_layout(PeBatch *B)
     int max_mat = 1;
     for (int s = 0; s < (int)B->solves.size(); ++s) {
         const PeConfig &c = B->solves[s]->cfg;
-        max_mat = std::max(max_mat, c.n_mat);
+        if (B->solves[s]->tma_capable) max_mat = std::max(max_mat, c.n_mat);
         const int target = c.z_chunk > 0 ? c.z_chunk : (B->z_chunk > 0 ? B->z_chunk : 40);
         const int nch = std::max(1, (c.nz + target - 1) / target);
         const int zc = (c.nz + nch - 1) / nch;
         B->solves[s]->zc_s = zc;
         B->solves[s]->zc_v = zc;
-        if (!B->solves[s]->tma_capable) continue;   // launched on its own
-        const int nzc = (c.nz + zc - 1) / zc;
-        for (int bz = 0; bz < nzc; ++bz) {
-            for (int by = 0; by < (c.ny + pe::TS_OY - 1) / pe::TS_OY; ++by)
-                for (int bx = 0; bx < (c.nx + pe::TS_OX - 1) / pe::TS_OX; ++bx) is.push_back({s, bx, by, bz});
-            for (int by = 0; by < (c.ny + pe::TB_Y - 1) / pe::TB_Y; ++by)
-                for (int bx = 0; bx < (c.nx + pe::TB_X - 1) / pe::TB_X; ++bx) iv.push_back({s, bx, by, bz});
-        }
     }
     int dev = 0, optin = 0, nsm = 148;
     PE_CUDA(cudaGetDevice(&dev));
@@ -952,13 +948,28 @@ int batch_layout(PeBatch *B)
     PE_CUDA(cudaFuncGetAttributes(&fa_s, pe::k_stress_tma_batch<T>));
     PE_CUDA(cudaFuncGetAttributes(&fa_v, pe::k_velocity_tma_batch<T>));
     const int dyn_s = optin - (int)fa_s.sharedSizeBytes, dyn_v = optin - (int)fa_v.sharedSizeBytes;
-    if (B->smem_s > (size_t)dyn_s || B->smem_v > (size_t)dyn_v)
-        return fail(PE_ERR_UNSUPPORTED, "material table too large for the batched kernels");
-    PE_CUDA(cudaFuncSetAttribute(pe::k_stress_tma_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_s));
-    PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_tma_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_v));
+    // when the batched kernels' tiles and tables do not fit (FP64 tiles with
+    // large tables), every solve runs its own launches instead
+    B->tma_batch = B->smem_s <= (size_t)dyn_s && B->smem_v <= (size_t)dyn_v;
     int per_s = 1, per_v = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, pe::k_stress_tma_batch<T>, pe::TB_N, B->smem_s);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_v, pe::k_velocity_tma_batch<T>, pe::TB_N, B->smem_v);
+    if (B->tma_batch) {
+        PE_CUDA(cudaFuncSetAttribute(pe::k_stress_tma_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_s));
+        PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_tma_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_v));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, pe::k_stress_tma_batch<T>, pe::TB_N, B->smem_s);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_v, pe::k_velocity_tma_batch<T>, pe::TB_N, B->smem_v);
+    }
+    for (int s = 0; s < (int)B->solves.size(); ++s) {
+        if (!batched(B, B->solves[s])) continue;   // launched on its own
+        const PeConfig &c = B->solves[s]->cfg;
+        const int zc = B->solves[s]->zc_s;
+        const int nzc = (c.nz + zc - 1) / zc;
+        for (int bz = 0; bz < nzc; ++bz) {
+            for (int by = 0; by < (c.ny + pe::TS_OY - 1) / pe::TS_OY; ++by)
+                for (int bx = 0; bx < (c.nx + pe::TS_OX - 1) / pe::TS_OX; ++bx) is.push_back({s, bx, by, bz});
+            for (int by = 0; by < (c.ny + pe::TB_Y - 1) / pe::TB_Y; ++by)
+                for (int bx = 0; bx < (c.nx + pe::TB_X - 1) / pe::TB_X; ++bx) iv.push_back({s, bx, by, bz});
+        }
+    }
     B->n_items_s = (int)is.size();
     B->n_items_v = (int)iv.size();
     B->grid_s = std::max(1, std::min(B->n_items_s, nsm * std::max(1, per_s)));
@@ -992,7 +1003,7 @@ int batch_upload(PeBatch *B, const PeState *states, void *const *traces)
         PeSolver *S = B->solves[s];
         int rc = ensure_maps(S, &states[s]);
         if (rc) return rc;
-        if (S->tma_capable && !S->tma)
+        if (batched(B, S) && !S->tma)
             return fail(PE_ERR_UNSUPPORTED, "batched solves need 16-byte aligned state buffers");
         descs[s] = make_args<T>(S, &states[s], 0);
         descs[s].step = B->step;
@@ -1026,11 +1037,12 @@ int batch_chunk(PeBatch *B, int len)
                 (const pe::StepArgs<T> *)B->descs, B->maps_v, B->nmats, B->items_v, B->n_items_v, k);
             B->launches += 2;
         }
-        // solves whose rows are not whole 16-byte units run the cp.async
-        // kernels, one launch pair each, on the same stream and step counter
+        // solves outside the batched launches (rows not whole 16-byte
+        // units, or tiles too large) run their own kernel pair each, on the
+        // same stream and step counter
         for (int s = 0; s < (int)B->solves.size(); ++s) {
             PeSolver *S = B->solves[s];
-            if (S->tma_capable) continue;
+            if (batched(B, S)) continue;
             pe::StepArgs<T> A = make_args<T>(S, &B->states[s], k);
             A.step = B->step;
             A.status = B->status;
