@@ -72,6 +72,21 @@ struct StepArgs {
 template <typename T>
 __device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
 
+// a / b for b > 0 (a face density), rounded as the plain division: a zero
+// numerator returns itself (+0 / b = +0, -0 / b = -0) without dividing.
+// Before the wavefront arrives most of the grid is zero, and profiling shows
+// zero numerators otherwise taking the division's slow path.
+template <typename T>
+__device__ __forceinline__ T div_face(T a, T b)
+{
+    T q = a;
+    if (a != T(0)) {
+        asm volatile("" ::: "memory");   // keeps the division inside the branch
+        q = a / b;
+    }
+    return q;
+}
+
 __device__ __forceinline__ int lower_bound_ll(const long long *a, int n, long long key)
 {
     int lo = 0, hi = n;
@@ -367,7 +382,7 @@ __global__ void __launch_bounds__(TX *TY) k_velocity(const StepArgs<T> A)
         const T rvz = (iz < nz - 1) ? T(0.5) * (r0 + ldg(A.rho + (A.lab[idx + sz] & LAB_MAT))) : r0;
         const T dmp = (T)damp_at(A, iz, iy, ix, idx);
         T tx = A.dt_h * ax, ty = A.dt_h * ay, tz = A.dt_h * az;
-        tx = tx / rvx; ty = ty / rvy; tz = tz / rvz;
+        tx = div_face(tx, rvx); ty = div_face(ty, rvy); tz = div_face(tz, rvz);
         const T vx = (A.v[0][idx] + tx) * dmp;
         const T vy = (A.v[1][idx] + ty) * dmp;
         const T vz = (A.v[2][idx] + tz) * dmp;

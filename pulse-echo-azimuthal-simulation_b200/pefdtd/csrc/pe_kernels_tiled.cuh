@@ -442,9 +442,9 @@ __device__ __forceinline__ void velocity_tiled_run(const StepArgs<T> &A, T *slot
             }
             const T dmp = (T)d;
             T ux = A.dt_h * ax, uy = A.dt_h * ay, uz = A.dt_h * az;
-            ux = ux / rvx;
-            uy = uy / rvy;
-            uz = uz / rvz;
+            ux = div_face(ux, rvx);
+            uy = div_face(uy, rvy);
+            uz = div_face(uz, rvz);
             const T vxn = (vc[0] + ux) * dmp;
             const T vyn = (vc[TB_N] + uy) * dmp;
             const T vzn = (vc[2 * TB_N] + uz) * dmp;

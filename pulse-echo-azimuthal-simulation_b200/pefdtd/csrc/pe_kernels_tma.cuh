@@ -494,9 +494,9 @@ __device__ __forceinline__ void velocity_tma_run(const TmapsVelocity &M, const S
             }
             const T dmp = (T)d;
             T ux = A.dt_h * ax, uy = A.dt_h * ay, uz = A.dt_h * az;
-            ux = ux / rvx;
-            uy = uy / rvy;
-            uz = uz / rvz;
+            ux = div_face(ux, rvx);
+            uy = div_face(uy, rvy);
+            uz = div_face(uz, rvz);
             const T vxn = (vc[0] + ux) * dmp;
             const T vyn = (vc[PC] + uy) * dmp;
             const T vzn = (vc[2 * PC] + uz) * dmp;
