@@ -305,13 +305,20 @@ def _device_budget(device=None):
 
 
 def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solver=None,
-        prefetch=True):
+        prefetch=True, rank=0, world=1):
     """Run (or continue) a sweep. ``batch``: azimuths per GPU batch (None =
     as many as fit in device memory). ``labeller``: see
     specimen.DiskSpecimen.build. ``solver``: callable(setups, progress) ->
     traces; the GPU batch solver unless replaced (tests drive the file
-    protocol on CPU with a stand-in)."""
+    protocol on CPU with a stand-in). ``rank``/``world``: one process per
+    GPU; each rank solves its share of the pending azimuths
+    (:func:`pefdtd.shard.assign`, every azimuth of a sweep costs the same)
+    and writes their files; rank 0 alone writes status.json."""
     root = _root_of(cfg, root)
+    if world > 1 and rank != 0:
+        status = lambda *a, **k: None  # noqa: E731,F841  (rank 0 owns status.json)
+    else:
+        status = globals()["status"]
     if solver is None:
         try:
             import torch
@@ -362,7 +369,11 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
         hb_stop.set()
     co = sweep_coeffs(cfg)
     todo = pending(cfg, root)
-    log(f"[sweep] {len(todo)} of {len(azimuths(cfg))} azimuths pending")
+    if world > 1:
+        from .shard import assign
+        todo = [todo[i] for i in assign([1.0] * len(todo), world)[rank]]
+    log(f"[sweep] {len(todo)} of {len(azimuths(cfg))} azimuths pending"
+        + (f" on rank {rank} of {world}" if world > 1 else ""))
     if not todo:
         status(cfg, root, phase="complete")
         return "complete"
