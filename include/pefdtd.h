@@ -71,9 +71,13 @@ typedef struct PeConfig {
     int32_t variant;        /* PeKernelVariant (0 = tiled, the default) */
 } PeConfig;
 
-/* Kernel family. Both are bit-identical; SIMPLE reads every tap through the
- * L1 cache and is kept as an independent cross-check of TILED. */
-enum PeKernelVariant { PE_KERNEL_TILED = 0, PE_KERNEL_SIMPLE = 1 };
+/* Kernel family; all are bit-identical. TILED picks the fastest tiled kernels
+ * the grid allows: in FP32 on grids whose rows are 16-byte multiples the
+ * pair-column kernels (each thread updates two x-adjacent cells), else the
+ * one-column tiled kernels. COLUMN forces the one-column tiled kernels and
+ * SIMPLE the untiled ones (every tap read through the L1 cache); both are
+ * kept as independent cross-checks of TILED. */
+enum PeKernelVariant { PE_KERNEL_TILED = 0, PE_KERNEL_SIMPLE = 1, PE_KERNEL_COLUMN = 2 };
 
 /* The medium. Volumes live on the device; tables are small host arrays. */
 typedef struct PeMedium {

@@ -1,0 +1,782 @@
+// Pair-column FP32 step kernels (the default FP32 path on grids whose rows
+// are 16-byte multiples).
+//
+// Arithmetic, term order and explicit FMA placement are those of the
+// one-column kernels (pe_kernels_tma.cuh, pe_kernels.cuh), so the results are
+// bit-identical to them and to the oracle. What changes is the number of
+// instructions spent per operand, which is what bounds the one-column
+// kernels: every thread owns two x-adjacent cells, so
+//  - each stencil tap read from shared memory is one 64-bit load serving
+//    both cells, and the x taps of a row (10 values) are five such loads;
+//  - the half-cell moves read strain rows as 64-bit pairs (42 loads per pair
+//    of cells instead of 156 scalar loads);
+//  - the stiffness product runs column by column (J outer), reading column J
+//    of a material from a shared-memory (n_mat, 36) table with one 128-bit
+//    and one 64-bit load per cell, which keeps the register footprint within
+//    the 512-thread budget;
+//  - tiles whose every tap lies inside the grid run an unguarded body; the
+//    others zero the coefficients of skipped taps instead of branching.
+// Data movement is the TMA scheme of the one-column kernels: one elected
+// thread issues cp.async.bulk.tensor box loads two planes ahead into three
+// mbarrier-tracked slots; z taps come from per-thread register rings.
+// Every mbarrier wait is bounded (status word, no hang).
+//
+// Block: 512 threads = 16 lanes along x (two columns each) x 32 rows.
+//   k_stress_pair    strain tile 32 x 32 columns, the inner 30 x 30 are
+//                    updated; replaces strains_zp + stress_lab_u + the source
+//                    scatter (sim/core/fdtd.py:1102-1177, :594-689,
+//                    :1798-1800).
+//   k_velocity_pair  32 x 32 cells; replaces vel_zp and the receiver gather
+//                    (sim/core/fdtd.py:1179-1257, :1806-1813).
+#pragma once
+#include "pe_kernels_tma.cuh"
+
+namespace pe {
+
+constexpr int PR_LX = 16, PR_ROWS = 32, PR_N = PR_LX * PR_ROWS;   // 512 threads
+// stress
+constexpr int PS_OX = 30, PS_OY = 30;                             // updated cells per block
+constexpr int PS_VW = 44, PS_VH = 40, PS_VSZ = PS_VW * PS_VH;     // v box: 1760 floats (7040 B)
+constexpr int PS_SW = 36, PS_SH = 30, PS_SSZ = PS_SW * PS_SH;     // cell box: 1080 floats
+constexpr int PS_SSZP = 1088;                                     // ... padded to 128 B
+constexpr int PS_GW = 32, PS_GOFF = 8, PS_GST = 1040;             // strain plane: pad, 32 x 32, pad
+constexpr int PS_VSLOT = 3 * PS_VSZ;
+constexpr int PS_SSLOT = 7 * PS_SSZP;
+// shared memory of a stress block: mbarriers (v, cell slot 0, cell slot 1),
+// one v slot, two cell slots, three strain planes, then the material table
+constexpr size_t PS_SMEM_FIXED = 128 + sizeof(float) * ((size_t)PS_VSLOT + 2 * (size_t)PS_SSLOT + (size_t)3 * 6 * PS_GST);
+constexpr int TAB36 = 36;   // material: columns J as [C0J..C3J] at 4J, then [C4J, C5J] at 24 + 2J
+// velocity
+constexpr int PV_OX = 32, PV_OY = 32;
+constexpr int PV_TW = 40, PV_TH = 40, PV_TSZ = PV_TW * PV_TH;     // s box with halo: 6400 B
+constexpr int PV_CSZ = PV_OX * PV_OY;                             // cell box: 4096 B
+constexpr int PV_SLOT = 5 * PV_TSZ + 4 * PV_CSZ;
+
+struct alignas(64) TmapsPairStress {
+    CUtensorMap vt[3];   // vx, vy, vz: box 44 x 40
+    CUtensorMap sc[6];   // s1..s6: box 36 x 30
+    CUtensorMap dv;      // damping volume: box 36 x 30
+};
+struct alignas(64) TmapsPairVelocity {
+    CUtensorMap st[5];   // s1, s2, s4, s5, s6: box 40 x 40
+    CUtensorMap vc[3];   // vx, vy, vz: box 32 x 32
+    CUtensorMap dv;      // damping volume: box 32 x 32
+};
+
+// the table goes to shared memory when it fits the 227 KB opt-in limit
+__host__ __device__ constexpr bool pair_tab_in_smem(int n_mat)
+{
+    return PS_SMEM_FIXED + (size_t)n_mat * TAB36 * sizeof(float) <= 232448;
+}
+__host__ __device__ constexpr size_t stress_pair_smem(int n_mat)
+{
+    return PS_SMEM_FIXED + (pair_tab_in_smem(n_mat) ? (size_t)n_mat * TAB36 * sizeof(float) : 0);
+}
+__host__ __device__ constexpr bool pair_rho_in_smem(int n_mat) { return n_mat <= 8192; }
+__host__ __device__ constexpr size_t velocity_pair_smem(int n_mat)
+{
+    return 128 + sizeof(float) * (3 * (size_t)PV_SLOT + (pair_rho_in_smem(n_mat) ? (size_t)n_mat : 0));
+}
+
+__device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float2 ldg2(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void stg2(float *p, float a, float b)
+{
+    *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+}
+__device__ __forceinline__ float pick(float2 v, int c) { return c ? v.y : v.x; }
+// streaming column loads for the z rings: read once, kept out of L1 so that
+// L1 holds the material table
+__device__ __forceinline__ float2 ldg2_stream(const float *p)
+{
+    float2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
+
+// ======================================================================== stress
+// Tap limits near the grid faces. The reference skips a tap whose reach
+// leaves the grid (sim/core/fdtd.py:1141-1162, :1215-1236): tap j of a
+// backward difference along x at column x exists iff j < min(x, nx - x), of
+// a forward difference iff j < min(x + 1, nx - x - 1). The guarded bodies
+// multiply instead of branching: a skipped tap gets the coefficient 0, and
+// fma(0, d, a) == a bit for bit for finite d, because an accumulator that
+// starts at +0 is never -0.
+struct TapLimits {
+    int xb[2], xf[2], yb, yf;
+};
+__device__ __forceinline__ int lim_b(int i, int n) { return min(i, n - i); }
+__device__ __forceinline__ int lim_f(int i, int n) { return min(i + 1, n - i - 1); }
+template <bool G>
+__device__ __forceinline__ float tapc(float cj, int j, int lim) { return (!G || j < lim) ? cj : 0.0f; }
+
+// strain of both columns at plane q; cv = this thread's cell 0 in the vx box
+template <int NC, bool G>
+__device__ __forceinline__ void pair_strain(const StepArgs<float> &A, int q, const float *cv,
+                                            const float (&rz)[2][8], const float (&ry)[2][8],
+                                            const float (&rx)[2][8], const TapLimits &tl,
+                                            float (&g)[2][6])
+{
+    constexpr int W = PS_VW;
+    const float *tvx = cv, *tvy = cv + PS_VSZ, *tvz = cv + 2 * PS_VSZ;
+    float X[10], Y[10], Z[10];   // centre rows, columns (cell 0) - 4 .. + 5
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const float2 a = lds2(tvx + 2 * k - 4), b = lds2(tvy + 2 * k - 4), c = lds2(tvz + 2 * k - 4);
+        X[2 * k] = a.x; X[2 * k + 1] = a.y;
+        Y[2 * k] = b.x; Y[2 * k + 1] = b.y;
+        Z[2 * k] = c.x; Z[2 * k + 1] = c.y;
+    }
+    float a1[2] = {0.f, 0.f}, a2[2] = {0.f, 0.f}, a3[2] = {0.f, 0.f};
+    float a4[2] = {0.f, 0.f}, a5[2] = {0.f, 0.f}, a6[2] = {0.f, 0.f};
+    const int nz = A.nz;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (NC ? j < NC : j < A.nc) {
+            const float cj = A.c[j];
+            const float czb = tapc<G>(cj, j, lim_b(q, nz)), czf = tapc<G>(cj, j, lim_f(q, nz));
+            const float cyb = tapc<G>(cj, j, tl.yb), cyf = tapc<G>(cj, j, tl.yf);
+            const float2 yp = lds2(tvy + j * W), ym = lds2(tvy - (j + 1) * W);     // Dby vy
+            const float2 zp = lds2(tvz + (j + 1) * W), zm = lds2(tvz - j * W);     // Dfy vz
+            const float2 xp = lds2(tvx + (j + 1) * W), xm = lds2(tvx - j * W);     // Dfy vx
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float cxb = tapc<G>(cj, j, tl.xb[c]), cxf = tapc<G>(cj, j, tl.xf[c]);
+                a1[c] = fmac(a1[c], cxb, X[4 + c + j] - X[3 + c - j]);
+                a2[c] = fmac(a2[c], cyb, pick(yp, c) - pick(ym, c));
+                a3[c] = fmac(a3[c], czb, rz[c][4 + j] - rz[c][3 - j]);
+                a4[c] = fmac(a4[c], cyf, pick(zp, c) - pick(zm, c));
+                a4[c] = fmac(a4[c], czf, ry[c][4 + j] - ry[c][3 - j]);
+                a5[c] = fmac(a5[c], cxf, Z[5 + c + j] - Z[4 + c - j]);
+                a5[c] = fmac(a5[c], czf, rx[c][4 + j] - rx[c][3 - j]);
+                a6[c] = fmac(a6[c], cxf, Y[5 + c + j] - Y[4 + c - j]);
+                a6[c] = fmac(a6[c], cyf, pick(xp, c) - pick(xm, c));
+            }
+        }
+    }
+    const float ih = A.inv_h;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        g[c][0] = a1[c] * ih; g[c][1] = a2[c] * ih; g[c][2] = a3[c] * ih;
+        g[c][3] = a4[c] * ih; g[c][4] = a5[c] * ih; g[c][5] = a6[c] * ih;
+    }
+}
+
+// strain J at (dz, dy) and column offset dx in -1..2 from cell 0; pl[k] is
+// the ring plane of dz = k - 1 at this thread's cell 0
+__device__ __forceinline__ float gval(const float *const (&pl)[3], int J, int dz, int dy, int dx)
+{
+    const float *p = pl[dz + 1] + J * PS_GST + dy * PS_GW + (dx & ~1);
+    const float2 v = lds2(p);
+    return (dx & 1) ? v.y : v.x;
+}
+
+struct MoveGuards {
+    bool zlo, zhi, ylo, yhi, xlo[2], xhi[2];
+};
+
+// strain J moved to position P (sim/core/fdtd.py:612-633) for both cells:
+// 4 taps summed z-major, times 1/4, zero where a needed neighbour is off
+// the grid; the term order of qval() in pe_kernels.cuh
+template <int P, int J, bool G>
+__device__ __forceinline__ void qpair(const float *const (&pl)[3], const MoveGuards &mg, float (&q)[2])
+{
+    constexpr int S = vpos(J);
+    constexpr int DZ = pos_z(P) - pos_z(S), DY = pos_y(P) - pos_y(S), DX = pos_x(P) - pos_x(S);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        if constexpr (DZ == 0 && DY == 0 && DX == 0) {
+            q[c] = gval(pl, J, 0, 0, c);
+        } else {
+            constexpr int LZ = DZ < 0 ? -1 : 0, HZ = DZ > 0 ? 1 : 0;
+            constexpr int LY = DY < 0 ? -1 : 0, HY = DY > 0 ? 1 : 0;
+            constexpr int LX = DX < 0 ? -1 : 0, HX = DX > 0 ? 1 : 0;
+            float acc = 0.f;
+            bool first = true;
+#pragma unroll
+            for (int a0 = LZ; a0 <= HZ; ++a0)
+#pragma unroll
+                for (int a1 = LY; a1 <= HY; ++a1)
+#pragma unroll
+                    for (int a2 = LX; a2 <= HX; ++a2) {
+                        const float t = gval(pl, J, a0, a1, c + a2);
+                        acc = first ? t : acc + t;
+                        first = false;
+                    }
+            if constexpr (G) {
+                bool ok = true;
+                if constexpr (DZ > 0) ok = ok && mg.zhi;
+                if constexpr (DZ < 0) ok = ok && mg.zlo;
+                if constexpr (DY > 0) ok = ok && mg.yhi;
+                if constexpr (DY < 0) ok = ok && mg.ylo;
+                if constexpr (DX > 0) ok = ok && mg.xhi[c];
+                if constexpr (DX < 0) ok = ok && mg.xlo[c];
+                q[c] = ok ? acc * 0.25f : 0.0f;
+            } else {
+                q[c] = acc * 0.25f;
+            }
+        }
+    }
+}
+
+// column J of the stiffness product: acc[I] = fmac(acc[I], C[I][J], q_J at
+// the position of stress I), J ascending as in row_dot(). TS: the table is
+// in shared memory (else global, through the read-only cache).
+template <int J, bool G, bool TS>
+__device__ __forceinline__ void stiff_column(const float *const (&pl)[3], const MoveGuards &mg,
+                                             const float *const (&crow)[2], float (&acc)[6][2])
+{
+    float q0[2], q1[2], q2[2], q3[2];
+    qpair<0, J, G>(pl, mg, q0);
+    qpair<1, J, G>(pl, mg, q1);
+    qpair<2, J, G>(pl, mg, q2);
+    qpair<3, J, G>(pl, mg, q3);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const float4 a = TS ? lds4(crow[c] + 4 * J) : ldg4(crow[c] + 4 * J);
+        const float2 b = TS ? lds2(crow[c] + 24 + 2 * J) : ldg2(crow[c] + 24 + 2 * J);
+        acc[0][c] = fmac(acc[0][c], a.x, q0[c]);
+        acc[1][c] = fmac(acc[1][c], a.y, q0[c]);
+        acc[2][c] = fmac(acc[2][c], a.z, q0[c]);
+        acc[3][c] = fmac(acc[3][c], a.w, q1[c]);
+        acc[4][c] = fmac(acc[4][c], b.x, q2[c]);
+        acc[5][c] = fmac(acc[5][c], b.y, q3[c]);
+    }
+}
+
+template <bool G, bool TS>
+__device__ __forceinline__ void stiff_all(const float *const (&pl)[3], const MoveGuards &mg,
+                                          const float *const (&crow)[2], float (&acc)[6][2])
+{
+#pragma unroll
+    for (int I = 0; I < 6; ++I) acc[I][0] = acc[I][1] = 0.f;
+    stiff_column<0, G, TS>(pl, mg, crow, acc);
+    stiff_column<1, G, TS>(pl, mg, crow, acc);
+    stiff_column<2, G, TS>(pl, mg, crow, acc);
+    stiff_column<3, G, TS>(pl, mg, crow, acc);
+    stiff_column<4, G, TS>(pl, mg, crow, acc);
+    stiff_column<5, G, TS>(pl, mg, crow, acc);
+}
+
+// mbarrier phase counters of a block, carried across its marches
+struct PairPhases {
+    int v, s;   // v loads / cell-box loads issued (and waited) so far
+};
+
+// One z-march of a block over strain tile (bx, by), updating planes
+// [zb, ze). tab: the (n_mat, 36) table (shared memory when TS). Pipeline per
+// iteration (strain plane q, update plane z = q - 1):
+//   wait v(q) | sync A | issue cell box z + 1 | strains of q | wait cell box z
+//   | sync B | issue v(q + 1) | updates of plane z
+// One v slot suffices (its refill overlaps the update phase); the cell boxes
+// alternate between two slots and are issued a plane ahead. The caller
+// synchronises the block before a march that follows another.
+template <int NC, bool TS>
+__device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, const StepArgs<float> &A,
+                                                  const float *tab, unsigned char *smem, int bx, int by,
+                                                  int zb, int ze, PairPhases &ph)
+{
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem);
+    float *vslot = reinterpret_cast<float *>(smem + 128);
+    float *sslots = vslot + PS_VSLOT;
+    float *gs = sslots + 2 * PS_SSLOT;
+    const int tid = threadIdx.x;
+    const int l = tid & (PR_LX - 1), r = tid >> 4;
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const long long sy = A.sy, sz = A.sz;
+    const int S0 = bx * PS_OX - 2, S0y = by * PS_OY - 1;   // first strain column / row (S0 even)
+    const int gx0 = S0 + 2 * l, gy = S0y + r;
+    const bool pair_ok = gx0 >= 0 && gx0 < nx && gy >= 0 && gy < ny;   // nx even: both columns
+    const int col = pair_ok ? (int)(gy * sy + gx0) : 0;
+    const long long n = *A.step + A.k;
+    const float wn = A.n_src ? A.wavelet[n] : 0.f;
+    const int xv = floor4(S0 - T_H), xs = floor4(S0);    // box x-origins (16-byte multiples)
+    const int q0 = zb - 1;
+    const bool has_dvol = A.dvol != nullptr;
+    const unsigned bytes_s = (6u * PS_SSZ + (has_dvol ? (unsigned)PS_SSZ : 0u)) * 4u;
+    const unsigned bytes_v = 3u * PS_VSZ * 4u;
+    const int v0 = ph.v, s0 = ph.s;   // phase counts at the start of this march
+
+    auto issue_v = [&](int q) {   // v boxes of plane q (q0 <= q <= ze)
+        fence_proxy_async();
+        mbar_expect_tx(bars, bytes_v);
+#pragma unroll
+        for (int f = 0; f < 3; ++f) tma_load_3d(vslot + f * PS_VSZ, &M.vt[f], xv, S0y - T_H, q, bars);
+    };
+    auto issue_s = [&](int z) {   // cell boxes of plane z (zb <= z < ze)
+        const int k = (s0 + z - zb) & 1;
+        unsigned long long *bar = bars + 1 + k;
+        float *ds = sslots + k * PS_SSLOT;
+        fence_proxy_async();
+        mbar_expect_tx(bar, bytes_s);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) tma_load_3d(ds + f * PS_SSZP, &M.sc[f], xs, S0y + 1, z, bar);
+        if (has_dvol) tma_load_3d(ds + 6 * PS_SSZP, &M.dv, xs, S0y + 1, z, bar);
+    };
+
+    // z rings (rz[c][k] <-> plane q-4+k, ry/rx[c][k] <-> q-3+k), one plane ahead
+    const float *pz = A.v[2] + col, *py = A.v[1] + col, *px = A.v[0] + col;
+    auto ld2col = [&](const float *f, int q) -> float2 {
+        return (pair_ok && q >= 0 && q < nz) ? ldg2_stream(f + (long long)q * sz) : make_float2(0.f, 0.f);
+    };
+    float rz[2][8], ry[2][8], rx[2][8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float2 a = ld2col(pz, q0 - 4 + k), b = ld2col(py, q0 - 3 + k), c = ld2col(px, q0 - 3 + k);
+        rz[0][k] = a.x; rz[1][k] = a.y;
+        ry[0][k] = b.x; ry[1][k] = b.y;
+        rx[0][k] = c.x; rx[1][k] = c.y;
+    }
+    TapLimits tl;
+    MoveGuards mg;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const int x = gx0 + c;
+        tl.xb[c] = lim_b(x, nx);
+        tl.xf[c] = lim_f(x, nx);
+        mg.xlo[c] = x >= 1;
+        mg.xhi[c] = x <= nx - 2;
+    }
+    tl.yb = lim_b(gy, ny);
+    tl.yf = lim_f(gy, ny);
+    mg.ylo = gy >= 1;
+    mg.yhi = gy <= ny - 2;
+    // updated cells: inner 30 x 30 of the strain tile, inside the grid
+    const bool row_out = r >= 1 && r <= PS_OY && gy < ny;
+    bool out_c[2];
+    out_c[0] = row_out && l >= 1 && gx0 >= 0 && gx0 < nx;
+    out_c[1] = row_out && l <= PR_LX - 2 && gx0 + 1 >= 0 && gx0 + 1 < nx;
+    const bool any_out = out_c[0] || out_c[1];
+    float dyx = 1.0f, dxx[2] = {1.0f, 1.0f};
+    if (A.dz && any_out) {
+        dyx = A.dy[gy];
+        dxx[0] = A.dx[gx0];
+        dxx[1] = A.dx[gx0 + 1];
+    }
+    const bool tile_in = S0 - T_H >= 0 && S0 + PS_GW - 1 + T_H < nx && S0y - T_H >= 0 &&
+                         S0y + PR_ROWS - 1 + T_H < ny;
+    const int cv = (r + T_H) * PS_VW + (S0 - xv) + 2 * l;   // cell 0 in a v box (even)
+    const int cs = (r - 1) * PS_SW + (S0 - xs) + 2 * l;     // cell 0 in a cell box (even)
+    const int cg = PS_GOFF + r * PS_GW + 2 * l;              // cell 0 in a strain plane
+    const uint32_t *lab32 = reinterpret_cast<const uint32_t *>(A.lab);
+    auto ldlab = [&](int z) -> uint32_t {
+        return (any_out && z >= zb && z < ze) ? __ldg(lab32 + (((long long)z * sz + col) >> 1)) : 0u;
+    };
+    uint32_t lab_next = 0u;
+    int *status = A.status;
+
+    if (tid == 0) {
+        issue_v(q0);
+        issue_s(zb);
+        if (zb + 1 < ze) issue_s(zb + 1);
+    }
+    const int n_it = ze - q0 + 1;
+    for (int i = 0; i < n_it; ++i) {
+        const int q = q0 + i;
+        const int sl = i % 3;   // strain ring slot of plane q
+        if (tid < 32) mbar_wait(bars, (unsigned)(v0 + i) & 1u, status);
+        __syncthreads();   // A: v(q) landed (observed by warp 0); the updates of plane q - 2 are done
+        if (tid == 0 && q >= zb + 2 && q < ze) issue_s(q);   // into the slot plane q - 2 used
+        const float2 nzv = ld2col(pz, q + 4), nyv = ld2col(py, q + 5), nxv = ld2col(px, q + 5);
+        const int z = q - 1;
+        const uint32_t lab2 = lab_next;
+        lab_next = ldlab(q);
+        const bool fast = NC == 4 && tile_in && q >= T_H && q <= nz - 1 - T_H;
+        {
+            const float *tv = vslot + cv;
+            float g[2][6];
+            if (fast) pair_strain<NC, false>(A, q, tv, rz, ry, rx, tl, g);
+            else pair_strain<NC, true>(A, q, tv, rz, ry, rx, tl, g);
+            float *gw = gs + sl * 6 * PS_GST + cg;
+#pragma unroll
+            for (int J = 0; J < 6; ++J) stg2(gw + J * PS_GST, g[0][J], g[1][J]);
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                rz[c][k] = rz[c][k + 1];
+                ry[c][k] = ry[c][k + 1];
+                rx[c][k] = rx[c][k + 1];
+            }
+        }
+        rz[0][7] = nzv.x; rz[1][7] = nzv.y;
+        ry[0][7] = nyv.x; ry[1][7] = nyv.y;
+        rx[0][7] = nxv.x; rx[1][7] = nxv.y;
+        const int us = s0 + z - zb;   // cell-box load index of plane z
+        if (tid < 32 && z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
+        __syncthreads();   // B: strains of q written; the v slot is free; cell box z landed
+        if (tid == 0 && q + 1 <= ze) issue_v(q + 1);
+        if (z >= zb && any_out) {
+            // strain planes z-1, z, z+1 were written at iterations i-2, i-1, i
+            const float *const pl[3] = {gs + ((i + 1) % 3) * 6 * PS_GST + cg,
+                                        gs + ((i + 2) % 3) * 6 * PS_GST + cg,
+                                        gs + sl * 6 * PS_GST + cg};
+            mg.zlo = z >= 1;
+            mg.zhi = z <= nz - 2;
+            const uint16_t lab[2] = {(uint16_t)(lab2 & 0xFFFFu), (uint16_t)(lab2 >> 16)};
+            const float *const crow[2] = {tab + (lab[0] & LAB_MAT) * TAB36, tab + (lab[1] & LAB_MAT) * TAB36};
+            float acc[6][2];
+            if (fast) stiff_all<false, TS>(pl, mg, crow, acc);
+            else stiff_all<true, TS>(pl, mg, crow, acc);
+            const float *sc = sslots + (us & 1) * PS_SSLOT + cs;
+            float dmp[2];
+            {
+                const float dz = A.dz ? A.dz[z] : 1.0f;
+                float2 dvv = make_float2(1.0f, 1.0f);
+                if (has_dvol) dvv = lds2(sc + 6 * PS_SSZP);
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    float d = 1.0f;
+                    if (A.dz) {
+                        d = dz * dyx;
+                        d = d * dxx[c];
+                    }
+                    if (has_dvol) d = A.dz ? d * pick(dvv, c) : pick(dvv, c);
+                    dmp[c] = d;
+                }
+            }
+            float sv[6][2];
+#pragma unroll
+            for (int I = 0; I < 6; ++I) {
+                const float2 so = lds2(sc + I * PS_SSZP);
+                sv[I][0] = fmac(so.x * dmp[0], A.dt, acc[I][0]);
+                sv[I][1] = fmac(so.y * dmp[1], A.dt, acc[I][1]);
+            }
+            const long long idx0 = (long long)z * sz + col;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (out_c[c] && (lab[c] & LAB_SRC)) {
+                    const long long idx = idx0 + c;
+                    const int e = lower_bound_ll(A.src_idx, A.n_src, idx);
+                    if (e < A.n_src && A.src_idx[e] == idx) {
+                        const float add = wn * A.src_w[e];
+                        sv[0][c] = sv[0][c] + add;
+                        sv[1][c] = sv[1][c] + add;
+                        sv[2][c] = sv[2][c] + add;
+                    }
+                }
+            }
+            if (out_c[0] && out_c[1]) {
+#pragma unroll
+                for (int I = 0; I < 6; ++I) stg2(A.s[I] + idx0, sv[I][0], sv[I][1]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (out_c[c]) {
+#pragma unroll
+                        for (int I = 0; I < 6; ++I) A.s[I][idx0 + c] = sv[I][c];
+                    }
+            }
+            if (A.rec_kind == 0) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (out_c[c] && (lab[c] & LAB_REC)) {
+                        float a = sv[0][c], b = sv[1][c], e = sv[2][c];
+                        if (A.rec_damped) { a = a * dmp[c]; b = b * dmp[c]; e = e * dmp[c]; }
+                        float t = a + b;
+                        t = t + e;
+                        record_cell(A, idx0 + c, -t / 3.0f);
+                    }
+                }
+            }
+        }
+    }
+    ph.v = v0 + n_it;
+    ph.s = s0 + (ze - zb);
+}
+
+// Stage the (n_mat, 36) table into shared memory (16-byte copies).
+__device__ __forceinline__ void stage_table(float *dst, const float *src, int n_mat)
+{
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+    for (int i = threadIdx.x; i < n_mat * (TAB36 / 4); i += blockDim.x) d4[i] = __ldg(s4 + i);
+}
+
+__device__ __forceinline__ void stress_pair_init(unsigned char *smem)
+{
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem);
+    float *gs = reinterpret_cast<float *>(smem + 128) + PS_VSLOT + 2 * PS_SSLOT;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 3; ++s) mbar_init(bars + s, 1);
+        fence_mbar_init();
+    }
+    // zero the strain planes' pads (read only by cells that are not updated)
+    for (int i = threadIdx.x; i < 3 * 6 * 2 * PS_GOFF; i += blockDim.x) {
+        const int p = i / (2 * PS_GOFF), k = i % (2 * PS_GOFF);
+        gs[p * PS_GST + (k < PS_GOFF ? k : PS_GST - 2 * PS_GOFF + k)] = 0.f;
+    }
+}
+
+// Launch grid: (tiles x, tiles y, z-chunks of A.zc planes). Blocks that run
+// at the same time march the same planes of neighbouring tiles, so the tile
+// halos they share are read from DRAM once and from L2 after that.
+template <int NC, bool TS>
+__global__ void __launch_bounds__(PR_N, 1) k_stress_pair(const __grid_constant__ TmapsPairStress M,
+                                                         const StepArgs<float> A,
+                                                         const float *__restrict__ tab36, int n_mat)
+{
+    extern __shared__ __align__(128) unsigned char smem_pair[];
+    float *tsm = reinterpret_cast<float *>(smem_pair + PS_SMEM_FIXED);
+    stress_pair_init(smem_pair);
+    if (TS) stage_table(tsm, tab36, n_mat);
+    __syncthreads();
+    const int zb = blockIdx.z * A.zc;
+    PairPhases ph{0, 0};
+    stress_pair_march<NC, TS>(M, A, TS ? tsm : tab36, smem_pair, blockIdx.x, blockIdx.y, zb,
+                              min(zb + A.zc, A.nz), ph);
+}
+
+// ====================================================================== velocity
+template <int NC, bool G>
+__device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, const float *t1,
+                                              const float *t2, const float *t4, const float *t5,
+                                              const float *t6, const float (&r3)[2][8],
+                                              const float (&r4)[2][8], const float (&r5)[2][8],
+                                              const TapLimits &tl, float (&ax)[2], float (&ay)[2],
+                                              float (&az)[2])
+{
+    constexpr int W = PV_TW;
+    float S1[10], S5[10], S6[10];   // centre rows, columns (cell 0) - 4 .. + 5
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const float2 a = lds2(t1 + 2 * k - 4), b = lds2(t5 + 2 * k - 4), c = lds2(t6 + 2 * k - 4);
+        S1[2 * k] = a.x; S1[2 * k + 1] = a.y;
+        S5[2 * k] = b.x; S5[2 * k + 1] = b.y;
+        S6[2 * k] = c.x; S6[2 * k + 1] = c.y;
+    }
+    const int nz = A.nz;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) ax[c] = ay[c] = az[c] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (NC ? j < NC : j < A.nc) {
+            const float cj = A.c[j];
+            const float2 p2 = lds2(t2 + (j + 1) * W), m2 = lds2(t2 - j * W);         // Dfy s2
+            const float2 p6 = lds2(t6 + j * W), m6 = lds2(t6 - (j + 1) * W);         // Dby s6
+            const float2 p4 = lds2(t4 + j * W), m4 = lds2(t4 - (j + 1) * W);         // Dby s4
+            const float czf = tapc<G>(cj, j, lim_f(z, nz)), czb = tapc<G>(cj, j, lim_b(z, nz));
+            const float cyf = tapc<G>(cj, j, tl.yf), cyb = tapc<G>(cj, j, tl.yb);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float cxb = tapc<G>(cj, j, tl.xb[c]), cxf = tapc<G>(cj, j, tl.xf[c]);
+                ax[c] = fmac(ax[c], cxf, S1[5 + c + j] - S1[4 + c - j]);
+                ay[c] = fmac(ay[c], cxb, S6[4 + c + j] - S6[3 + c - j]);
+                az[c] = fmac(az[c], cxb, S5[4 + c + j] - S5[3 + c - j]);
+                ay[c] = fmac(ay[c], cyf, pick(p2, c) - pick(m2, c));
+                ax[c] = fmac(ax[c], cyb, pick(p6, c) - pick(m6, c));
+                az[c] = fmac(az[c], cyb, pick(p4, c) - pick(m4, c));
+                az[c] = fmac(az[c], czf, r3[c][4 + j] - r3[c][3 - j]);
+                ax[c] = fmac(ax[c], czb, r5[c][4 + j] - r5[c][3 - j]);
+                ay[c] = fmac(ay[c], czb, r4[c][4 + j] - r4[c][3 - j]);
+            }
+        }
+    }
+}
+
+// One z-march of a block over cell tile (bx, by), planes [zb, ze); it0 as
+// in stress_pair_march.
+template <int NC>
+__device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, const StepArgs<float> &A,
+                                                   const float *rho_tab, unsigned char *smem, int bx,
+                                                   int by, int zb, int ze, int it0)
+{
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem);
+    float *slots = reinterpret_cast<float *>(smem + 128);
+    const int tid = threadIdx.x;
+    const int l = tid & (PR_LX - 1), r = tid >> 4;
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const long long sy = A.sy, sz = A.sz;
+    const int x0 = bx * PV_OX, y0 = by * PV_OY;
+    const int ix = x0 + 2 * l, iy = y0 + r;
+    const bool out_ok = ix < nx && iy < ny;   // nx even: both cells
+    const int col = out_ok ? (int)(iy * sy + ix) : 0;
+    const bool has_dvol = A.dvol != nullptr;
+    const unsigned bytes = (5u * PV_TSZ + 3u * PV_CSZ + (has_dvol ? (unsigned)PV_CSZ : 0u)) * 4u;
+
+    auto issue = [&](int i) {
+        const int z = zb + i;
+        if (tid != 0 || z >= ze) return;
+        const int sl = (it0 + i) % 3;
+        unsigned long long *bar = bars + sl;
+        float *d = slots + sl * PV_SLOT;
+        fence_proxy_async();
+        mbar_expect_tx(bar, bytes);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) tma_load_3d(d + f * PV_TSZ, &M.st[f], x0 - T_H, y0 - T_H, z, bar);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tma_load_3d(d + 5 * PV_TSZ + c * PV_CSZ, &M.vc[c], x0, y0, z, bar);
+        if (has_dvol) tma_load_3d(d + 5 * PV_TSZ + 3 * PV_CSZ, &M.dv, x0, y0, z, bar);
+    };
+    const float *p3 = A.s[2] + col, *p4 = A.s[3] + col, *p5 = A.s[4] + col;
+    auto ld2col = [&](const float *f, int z) -> float2 {
+        return (out_ok && z >= 0 && z < nz) ? ldg2_stream(f + (long long)z * sz) : make_float2(0.f, 0.f);
+    };
+    float r3[2][8], r4[2][8], r5[2][8];   // r3[c][k] <-> z-3+k, r4/r5[c][k] <-> z-4+k
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float2 a = ld2col(p3, zb - 3 + k), b = ld2col(p4, zb - 4 + k), c = ld2col(p5, zb - 4 + k);
+        r3[0][k] = a.x; r3[1][k] = a.y;
+        r4[0][k] = b.x; r4[1][k] = b.y;
+        r5[0][k] = c.x; r5[1][k] = c.y;
+    }
+    TapLimits tl;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        tl.xb[c] = lim_b(ix + c, nx);
+        tl.xf[c] = lim_f(ix + c, nx);
+    }
+    tl.yb = lim_b(iy, ny);
+    tl.yf = lim_f(iy, ny);
+    const bool xin1 = ix + 1 < nx - 1;   // cell 1 has a +x neighbour (cell 0 always does)
+    const bool yin = iy < ny - 1;
+    float dyx = 1.0f, dxx[2] = {1.0f, 1.0f};
+    if (A.dz && out_ok) {
+        dyx = A.dy[iy];
+        dxx[0] = A.dx[ix];
+        dxx[1] = A.dx[ix + 1];
+    }
+    const bool tile_in = x0 - T_H >= 0 && x0 + PV_OX - 1 + T_H < nx && y0 - T_H >= 0 &&
+                         y0 + PV_OY - 1 + T_H < ny;
+    const int tc = (r + T_H) * PV_TW + 2 * l + T_H;
+    const int cc = r * PV_OX + 2 * l;
+    const uint32_t *lab32 = reinterpret_cast<const uint32_t *>(A.lab);
+    // labels of plane z: the pair, cell x+2, and the pair at y+1
+    auto ldlabs = [&](int z, uint32_t &pr, uint16_t &px2, uint32_t &py) {
+        pr = 0u; px2 = 0; py = 0u;
+        if (out_ok && z < nz) {
+            const long long b = (long long)z * sz + col;
+            pr = __ldg(lab32 + (b >> 1));
+            if (xin1) px2 = A.lab[b + 2];
+            if (yin) py = __ldg(lab32 + ((b + sy) >> 1));
+        }
+    };
+    uint32_t lab_c, lab_y, nlab_c, nlab_y;
+    uint16_t lab_x2, nlab_x2;
+    ldlabs(zb, lab_c, lab_x2, lab_y);
+    ldlabs(zb + 1, nlab_c, nlab_x2, nlab_y);
+    int *status = A.status;
+
+    issue(0);
+    issue(1);
+    for (int i = 0; i < ze - zb; ++i) {
+        const int z = zb + i;
+        const int g = it0 + i, sl = g % 3;
+        if (tid < 32) mbar_wait(bars + sl, (unsigned)(g / 3) & 1u, status);
+        __syncthreads();   // slot g landed (observed by warp 0); slot g + 2 is free
+        issue(i + 2);
+        const float2 n3 = ld2col(p3, z + 5), n4 = ld2col(p4, z + 4), n5 = ld2col(p5, z + 4);
+        uint32_t mlab_c, mlab_y;
+        uint16_t mlab_x2;
+        ldlabs(z + 2, mlab_c, mlab_x2, mlab_y);
+        const float *slot = slots + sl * PV_SLOT;
+        const float *t = slot + tc;
+        float ax[2], ay[2], az[2];
+        const bool fast = NC == 4 && tile_in && z >= T_H && z <= nz - 1 - T_H;
+        if (fast) pair_vel_taps<NC, false>(A, z, t, t + PV_TSZ, t + 2 * PV_TSZ, t + 3 * PV_TSZ, t + 4 * PV_TSZ, r3, r4, r5, tl, ax, ay, az);
+        else pair_vel_taps<NC, true>(A, z, t, t + PV_TSZ, t + 2 * PV_TSZ, t + 3 * PV_TSZ, t + 4 * PV_TSZ, r3, r4, r5, tl, ax, ay, az);
+        if (out_ok) {
+            const uint16_t lc[2] = {(uint16_t)(lab_c & 0xFFFFu), (uint16_t)(lab_c >> 16)};
+            const uint16_t lyv[2] = {(uint16_t)(lab_y & 0xFFFFu), (uint16_t)(lab_y >> 16)};
+            const uint16_t lzv[2] = {(uint16_t)(nlab_c & 0xFFFFu), (uint16_t)(nlab_c >> 16)};
+            const uint16_t lxv[2] = {lc[1], lab_x2};
+            const float *vc = slot + 5 * PV_TSZ + cc;
+            float dmp[2];
+            {
+                const float dz = A.dz ? A.dz[z] : 1.0f;
+                float2 dvv = make_float2(1.0f, 1.0f);
+                if (has_dvol) dvv = lds2(vc + 3 * PV_CSZ);
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    float d = 1.0f;
+                    if (A.dz) {
+                        d = dz * dyx;
+                        d = d * dxx[c];
+                    }
+                    if (has_dvol) d = A.dz ? d * pick(dvv, c) : pick(dvv, c);
+                    dmp[c] = d;
+                }
+            }
+            const float2 vxo = lds2(vc), vyo = lds2(vc + PV_CSZ), vzo = lds2(vc + 2 * PV_CSZ);
+            float vn[3][2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const bool xin = c == 0 ? true : xin1;
+                const float r0 = rho_tab[lc[c] & LAB_MAT];
+                const float rvx = xin ? 0.5f * (r0 + rho_tab[lxv[c] & LAB_MAT]) : r0;
+                const float rvy = yin ? 0.5f * (r0 + rho_tab[lyv[c] & LAB_MAT]) : r0;
+                const float rvz = (z < nz - 1) ? 0.5f * (r0 + rho_tab[lzv[c] & LAB_MAT]) : r0;
+                float ux = A.dt_h * ax[c], uy = A.dt_h * ay[c], uz = A.dt_h * az[c];
+                ux = div_face(ux, rvx);
+                uy = div_face(uy, rvy);
+                uz = div_face(uz, rvz);
+                vn[0][c] = (pick(vxo, c) + ux) * dmp[c];
+                vn[1][c] = (pick(vyo, c) + uy) * dmp[c];
+                vn[2][c] = (pick(vzo, c) + uz) * dmp[c];
+            }
+            const long long idx = (long long)z * sz + col;
+            stg2(A.v[0] + idx, vn[0][0], vn[0][1]);
+            stg2(A.v[1] + idx, vn[1][0], vn[1][1]);
+            stg2(A.v[2] + idx, vn[2][0], vn[2][1]);
+            if (A.rec_kind != 0) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (lc[c] & LAB_REC)
+                        record_cell(A, idx + c, A.rec_kind == 1 ? vn[0][c] : (A.rec_kind == 2 ? vn[1][c] : vn[2][c]));
+            }
+        }
+        lab_c = nlab_c; lab_x2 = nlab_x2; lab_y = nlab_y;
+        nlab_c = mlab_c; nlab_x2 = mlab_x2; nlab_y = mlab_y;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                r3[c][k] = r3[c][k + 1];
+                r4[c][k] = r4[c][k + 1];
+                r5[c][k] = r5[c][k + 1];
+            }
+        }
+        r3[0][7] = n3.x; r3[1][7] = n3.y;
+        r4[0][7] = n4.x; r4[1][7] = n4.y;
+        r5[0][7] = n5.x; r5[1][7] = n5.y;
+    }
+    return ze - zb;
+}
+
+template <int NC>
+__global__ void __launch_bounds__(PR_N, 1) k_velocity_pair(const __grid_constant__ TmapsPairVelocity M,
+                                                           const StepArgs<float> A, int n_mat)
+{
+    extern __shared__ __align__(128) unsigned char smem_pair[];
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_pair);
+    float *rsm = reinterpret_cast<float *>(smem_pair + 128) + 3 * PV_SLOT;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < 3; ++s) mbar_init(bars + s, 1);
+        fence_mbar_init();
+    }
+    const bool rho_smem = pair_rho_in_smem(n_mat);
+    if (rho_smem)
+        for (int i = tid; i < n_mat; i += PR_N) rsm[i] = A.rho[i];
+    __syncthreads();
+    const float *rho_tab = rho_smem ? rsm : A.rho;
+    const int zb = blockIdx.z * A.zc;
+    velocity_pair_march<NC>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, min(zb + A.zc, A.nz), 0);
+}
+
+// (n_mat, 36) column-split stiffness from the (n_mat, 24) upper-triangle
+// rows, with C[I][J] as row_dot() reads it: tab[m][4J + I] for I < 4,
+// tab[m][24 + 2J + I - 4] for I = 4, 5
+__global__ void k_c21_to_tab36(const float *c21, float *tab, int n_mat)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_mat) return;
+    for (int J = 0; J < 6; ++J)
+        for (int I = 0; I < 6; ++I)
+            tab[m * TAB36 + (I < 4 ? 4 * J + I : 24 + 2 * J + I - 4)] = c21[m * C21_STRIDE + c21_slot(I, J)];
+}
+
+}  // namespace pe

@@ -14,11 +14,13 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "pe_kernels.cuh"
 #include "pe_kernels_tiled.cuh"
 #include "pe_kernels_tma.cuh"
+#include "pe_kernels_pair.cuh"
 #include "pe_adjoint.cuh"
 #include "pefdtd.h"
 
@@ -99,6 +101,13 @@ struct PeSolver {
     bool maps_ok = false;
     pe::TmapsStress ms{};
     pe::TmapsVelocity mv{};
+    // FP32 pair-column kernels (the default where the grid allows them)
+    float *tab36 = nullptr;     // (n_mat, 36) column-split stiffness
+    bool pair_capable = false;  // FP32, rows of 16-byte multiples, maps encodable, smem fits
+    bool pair = false;          // pair kernels in use for the current state
+    int zc_ps = 0, zc_pv = 0;   // planes per z-march of the pair launches
+    pe::TmapsPairStress mps{};
+    pe::TmapsPairVelocity mpv{};
 
     ~PeSolver()
     {
@@ -107,7 +116,7 @@ struct PeSolver {
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
         void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
-                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group};
+                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group, tab36};
         for (void *b : bufs)
             if (b) cudaFree(b);
     }
@@ -179,6 +188,21 @@ void launch_stress(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st
         return;
     }
     pe::StepArgs<T> A = A0;
+    if constexpr (std::is_same<T, float>::value) {
+        if (S->pair) {
+            A.zc = S->zc_ps;
+            // stress tiles update columns [30 bx - 1, 30 bx + 29)
+            dim3 grid((A.nx + pe::PS_OX) / pe::PS_OX, (A.ny + pe::PS_OY - 1) / pe::PS_OY, (A.nz + A.zc - 1) / A.zc);
+            const int nm = S->cfg.n_mat;
+            const size_t sm = pe::stress_pair_smem(nm);
+            const bool ts = pe::pair_tab_in_smem(nm);
+            if (A.nc == 4 && ts) pe::k_stress_pair<4, true><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            else if (A.nc == 4) pe::k_stress_pair<4, false><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            else if (ts) pe::k_stress_pair<0, true><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            else pe::k_stress_pair<0, false><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            return;
+        }
+    }
     A.zc = S->zc_s;
     dim3 grid((A.nx + pe::TS_OX - 1) / pe::TS_OX, (A.ny + pe::TS_OY - 1) / pe::TS_OY,
               (A.nz + A.zc - 1) / A.zc);
@@ -200,6 +224,18 @@ void launch_velocity(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t 
         return;
     }
     pe::StepArgs<T> A = A0;
+    if constexpr (std::is_same<T, float>::value) {
+        if (S->pair) {
+            A.zc = S->zc_pv;
+            dim3 grid((A.nx + pe::PV_OX - 1) / pe::PV_OX, (A.ny + pe::PV_OY - 1) / pe::PV_OY, (A.nz + A.zc - 1) / A.zc);
+            const size_t sm = pe::velocity_pair_smem(S->cfg.n_mat);
+            if (A.nc == 4)
+                pe::k_velocity_pair<4><<<grid, pe::PR_N, sm, st>>>(S->mpv, A, S->cfg.n_mat);
+            else
+                pe::k_velocity_pair<0><<<grid, pe::PR_N, sm, st>>>(S->mpv, A, S->cfg.n_mat);
+            return;
+        }
+    }
     A.zc = S->zc_v;
     dim3 grid((A.nx + pe::TB_X - 1) / pe::TB_X, (A.ny + pe::TB_Y - 1) / pe::TB_Y,
               (A.nz + A.zc - 1) / A.zc);
@@ -357,6 +393,25 @@ int configure_kernels(PeSolver *S)
     }
     S->zc_s = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, ts, ss, 4);
     S->zc_v = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tv, sv, 3);
+    if constexpr (std::is_same<T, float>::value) {
+        const size_t ps = pe::stress_pair_smem(c.n_mat), pv = pe::velocity_pair_smem(c.n_mat);
+        S->pair_capable = S->variant == PE_KERNEL_TILED && c.nx % 4 == 0 && ps <= (size_t)optin &&
+                          pv <= (size_t)optin && encode_fn() != nullptr;
+        if (S->pair_capable) {
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pv));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pv));
+            const long long tps = (long long)((c.nx + pe::PS_OX) / pe::PS_OX) * ((c.ny + pe::PS_OY - 1) / pe::PS_OY);
+            const long long tpv = (long long)((c.nx + pe::PV_OX - 1) / pe::PV_OX) * ((c.ny + pe::PV_OY - 1) / pe::PV_OY);
+            const int sps = occupancy_slots(pe::k_stress_pair<4, true>, pe::PR_N, ps);
+            const int spv = occupancy_slots(pe::k_velocity_pair<4>, pe::PR_N, pv);
+            S->zc_ps = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tps, sps, 3);
+            S->zc_pv = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tpv, spv, 2);
+        }
+    }
     return PE_OK;
 }
 
@@ -365,8 +420,9 @@ int configure_kernels(PeSolver *S)
 // to the cp.async kernels when a buffer is not 16-byte aligned.
 int ensure_maps(PeSolver *S, const PeState *st)
 {
-    if (!S->tma_capable) {
+    if (!S->tma_capable && !S->pair_capable) {
         S->tma = false;
+        S->pair = false;
         return PE_OK;
     }
     if (S->maps_ok && same_state(S->mstate, *st)) return PE_OK;
@@ -377,10 +433,30 @@ int ensure_maps(PeSolver *S, const PeState *st)
     for (int i = 0; i < 6; ++i) aligned = aligned && ((uintptr_t)st->s[i] % 16) == 0;
     S->mstate = *st;
     S->maps_ok = true;
-    S->tma = aligned;
+    S->tma = aligned && S->tma_capable;
+    S->pair = aligned && S->pair_capable;
     if (!aligned) return PE_OK;
     const CUtensorMapDataType dt = es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     int rc;
+    if (S->pair) {
+        for (int f = 0; f < 3; ++f)
+            if ((rc = encode_box(&S->mps.vt[f], st->v[f], dt, es, c, pe::PS_VW, pe::PS_VH))) return rc;
+        for (int f = 0; f < 6; ++f)
+            if ((rc = encode_box(&S->mps.sc[f], st->s[f], dt, es, c, pe::PS_SW, pe::PS_SH))) return rc;
+        const int pvf[5] = {0, 1, 3, 4, 5};
+        for (int f = 0; f < 5; ++f)
+            if ((rc = encode_box(&S->mpv.st[f], st->s[pvf[f]], dt, es, c, pe::PV_TW, pe::PV_TH))) return rc;
+        for (int f = 0; f < 3; ++f)
+            if ((rc = encode_box(&S->mpv.vc[f], st->v[f], dt, es, c, pe::PV_OX, pe::PV_OY))) return rc;
+        if (S->dvol) {
+            if ((rc = encode_box(&S->mps.dv, S->dvol, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c, pe::PS_SW, pe::PS_SH))) return rc;
+            if ((rc = encode_box(&S->mpv.dv, S->dvol, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c, pe::PV_OX, pe::PV_OY))) return rc;
+        } else {
+            std::memset(&S->mps.dv, 0, sizeof(S->mps.dv));
+            std::memset(&S->mpv.dv, 0, sizeof(S->mpv.dv));
+        }
+    }
+    if (!S->tma) return PE_OK;
     for (int f = 0; f < 3; ++f)
         if ((rc = encode_box(&S->ms.vt[f], st->v[f], dt, es, c, pe::KS_VW, pe::KS_VH))) return rc;
     for (int f = 0; f < 6; ++f)
@@ -441,8 +517,8 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     S->ncell = (long long)c.nz * c.ny * c.nx;
     S->esize = dtype_size(c.dtype);
     S->chunk = c.chunk_steps > 0 ? c.chunk_steps : 200;
-    if (c.variant != PE_KERNEL_TILED && c.variant != PE_KERNEL_SIMPLE)
-        return fail(PE_ERR_INVALID, "variant must be PE_KERNEL_TILED or PE_KERNEL_SIMPLE");
+    if (c.variant != PE_KERNEL_TILED && c.variant != PE_KERNEL_SIMPLE && c.variant != PE_KERNEL_COLUMN)
+        return fail(PE_ERR_INVALID, "variant must be PE_KERNEL_TILED, PE_KERNEL_SIMPLE or PE_KERNEL_COLUMN");
     S->variant = c.variant;
     if (c.tile_x > 0 && c.tile_y > 0) {
         const TileShape ok[] = {{32, 8}, {32, 4}};
@@ -541,6 +617,10 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
         else
             pe::k_c36_to_c21<float><<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)c36, (float *)S->c21, c.n_mat);
         PE_CUDA(cudaMemcpyAsync(S->rho, md->rho, (size_t)es * c.n_mat, cudaMemcpyHostToDevice, st));
+        if (c.dtype == PE_F32) {
+            if ((rc = dev_alloc(&S->tab36, sizeof(float) * pe::TAB36 * c.n_mat))) return rc;
+            pe::k_c21_to_tab36<<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)S->c21, S->tab36, c.n_mat);
+        }
         PE_CUDA(cudaStreamSynchronize(st));
         cudaFree(c36);
     }

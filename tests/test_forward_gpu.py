@@ -80,6 +80,8 @@ def test_bit_exact_vs_oracle_f64_and_f32_error(shape):
     ((23, 45, 68), (0, 0), 0, 11, "tiled"),
     ((19, 71, 132), (0, 0), 6, 200, "tiled"),
     ((9, 8, 4), (0, 0), 0, 0, "tiled"),
+    ((23, 45, 68), (0, 0), 0, 11, "column"),
+    ((19, 71, 132), (0, 0), 6, 200, "column"),
 ])
 def test_odd_grids_tiles_and_schedules(shape, tile, zc, chunk, variant):
     p = make_small(nt=60, shape=shape, n_grains=7, sponge=2) if min(shape) > 8 else _tiny(shape)
@@ -90,6 +92,31 @@ def test_odd_grids_tiles_and_schedules(shape, tile, zc, chunk, variant):
     ref = O.run_oracle(oracle_prob(p, record="pressure", damped_record=True, damp_mask=mask),
                        fma_mode=1)
     assert np.array_equal(tr, ref)
+
+
+@pytest.mark.parametrize("shape,order,zc,record,grains", [
+    ((24, 100, 104), 8, 0, "pressure", 9),   # interior tiles: unguarded bodies of both kernels
+    ((30, 72, 68), 6, 7, "vz", 9),           # runtime tap count
+    ((12, 36, 36), 2, 0, "vx", 9),
+    ((40, 9, 100), 8, 13, "vy", 9),
+    ((13, 66, 64), 4, 5, "pressure", 9),
+    ((18, 72, 72), 8, 0, "vz", 700),         # table too large for shared memory: read from L1/L2
+])
+def test_pair_kernels_bit_exact(shape, order, zc, record, grains):
+    """The FP32 pair-column kernels (default on rows of 16-byte multiples) are
+    bit-identical to the oracle and to the one-column kernels."""
+    from pefdtd import damping
+    from pefdtd.coeffs import optimised_coeffs
+    p = dict(make_small(nt=70, shape=shape, n_grains=grains, sponge=3))
+    assert len(p["rho_t"]) == p["n_grains"] + 1
+    p["coeffs"] = optimised_coeffs(order)
+    mask = damping.fluid_damp_mask(p["lab"], 0.05)
+    tr = _fwd(p, record=record, damp_mask=mask, damped_record=True, z_chunk=zc)
+    col = _fwd(p, record=record, damp_mask=mask, damped_record=True, z_chunk=zc, variant="column")
+    ref = O.run_oracle(oracle_prob(p, record=record, damped_record=True, damp_mask=mask), fma_mode=1)
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(tr, ref), f"max |diff| {np.abs(tr - ref).max()}"
+    assert np.array_equal(tr, col)
 
 
 def test_vs_reference_own_kernels_rel_l2():
