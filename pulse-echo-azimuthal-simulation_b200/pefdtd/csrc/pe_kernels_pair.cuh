@@ -767,6 +767,76 @@ __global__ void __launch_bounds__(PR_N, 1) k_velocity_pair(const __grid_constant
     velocity_pair_march<NC>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, min(zb + A.zc, A.nz), 0);
 }
 
+// ---------------------------------------------------------------- batches
+// Many solves (any grid sizes) advance one step per launch pair. Work items
+// (solve, tile x, tile y, z-chunk) are listed solve by solve and chunk-major
+// within a solve, so blocks that run together march the same planes of
+// neighbouring tiles; each resident block walks a contiguous run of items,
+// re-staging the solve's arguments and tables only when the solve changes.
+// All solves of a pair batch have rows of 16-byte multiples.
+template <int NC, bool TS>
+__global__ void __launch_bounds__(PR_N, 1)
+    k_stress_pair_batch(const StepArgs<float> *__restrict__ descs, const TmapsPairStress *__restrict__ maps,
+                        const float *const *__restrict__ tabs, const int *__restrict__ n_mats,
+                        const BatchItem *__restrict__ items, int n_items, int k)
+{
+    extern __shared__ __align__(128) unsigned char smem_pair[];
+    __shared__ __align__(16) StepArgs<float> As;
+    float *tsm = reinterpret_cast<float *>(smem_pair + PS_SMEM_FIXED);
+    stress_pair_init(smem_pair);
+    const int per = (n_items + gridDim.x - 1) / gridDim.x;
+    const int i0 = blockIdx.x * per, i1 = min(n_items, i0 + per);
+    int cur = -1;
+    PairPhases ph{0, 0};
+    for (int it = i0; it < i1; ++it) {
+        const BatchItem w = items[it];
+        __syncthreads();   // the previous march is finished by every thread
+        const bool fresh = w.solve != cur;
+        if (fresh) {
+            copy_args(&As, descs + w.solve, k);
+            if (TS) stage_table(tsm, tabs[w.solve], n_mats[w.solve]);
+        }
+        __syncthreads();
+        const int zb = w.bz * As.zc;
+        stress_pair_march<NC, TS>(maps[w.solve], As, TS ? tsm : tabs[w.solve], smem_pair, w.bx, w.by, zb,
+                                  min(zb + As.zc, As.nz), ph);
+        cur = w.solve;
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(PR_N, 1)
+    k_velocity_pair_batch(const StepArgs<float> *__restrict__ descs, const TmapsPairVelocity *__restrict__ maps,
+                          const int *__restrict__ n_mats, const BatchItem *__restrict__ items, int n_items,
+                          int k)
+{
+    extern __shared__ __align__(128) unsigned char smem_pair[];
+    __shared__ __align__(16) StepArgs<float> As;
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_pair);
+    float *rsm = reinterpret_cast<float *>(smem_pair + 128) + 3 * PV_SLOT;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 3; ++s) mbar_init(bars + s, 1);
+        fence_mbar_init();
+    }
+    const int per = (n_items + gridDim.x - 1) / gridDim.x;
+    const int i0 = blockIdx.x * per, i1 = min(n_items, i0 + per);
+    int cur = -1, it0 = 0;
+    for (int it = i0; it < i1; ++it) {
+        const BatchItem w = items[it];
+        __syncthreads();
+        const bool fresh = w.solve != cur;
+        if (fresh) {
+            copy_args(&As, descs + w.solve, k);
+            for (int i = threadIdx.x; i < n_mats[w.solve]; i += PR_N) rsm[i] = As.rho[i];
+        }
+        __syncthreads();
+        const int zb = w.bz * As.zc;
+        it0 += velocity_pair_march<NC>(maps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, min(zb + As.zc, As.nz),
+                                       it0);
+        cur = w.solve;
+    }
+}
+
 // (n_mat, 36) column-split stiffness from the (n_mat, 24) upper-triangle
 // rows, with C[I][J] as row_dot() reads it: tab[m][4J + I] for I < 4,
 // tab[m][24 + 2J + I - 4] for I = 4, 5

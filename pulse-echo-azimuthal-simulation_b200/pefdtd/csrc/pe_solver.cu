@@ -984,13 +984,21 @@ struct PeBatch {
     long long launches = 0;
     long long graph_launches = 0;   // kernels in one captured chunk
     bool tma_batch = true;          // the batched TMA kernels fit this batch
+    // FP32 batches of solves whose rows are 16-byte multiples run the
+    // pair-column kernels
+    bool pair_batch = false;
+    bool pair_ts = false;           // every batched table fits shared memory
+    bool pair_nc4 = true;           // every batched solve has four coefficients
+    pe::TmapsPairStress *pmaps_s = nullptr;
+    pe::TmapsPairVelocity *pmaps_v = nullptr;
+    const float **tabs = nullptr;
 
     ~PeBatch()
     {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (stream) cudaStreamSynchronize(stream);
         for (PeSolver *s : solves) pe_solver_destroy(s);
-        void *bufs[] = {step, status, descs, maps_s, maps_v, nmats, items_s, items_v};
+        void *bufs[] = {step, status, descs, maps_s, maps_v, nmats, items_s, items_v, pmaps_s, pmaps_v, tabs};
         for (void *b : bufs)
             if (b) cudaFree(b);
         if (ev_in) cudaEventDestroy(ev_in);
@@ -1002,7 +1010,56 @@ struct PeBatch {
 namespace {
 
 // Whether solve S runs inside the batched TMA launches (else its own pair).
-bool batched(const PeBatch *B, const PeSolver *S) { return B->tma_batch && S->tma_capable; }
+bool batched(const PeBatch *B, const PeSolver *S)
+{
+    return B->pair_batch ? S->pair_capable : (B->tma_batch && S->tma_capable);
+}
+
+// Pair-kernel layout of an FP32 batch: work items, grids and shared memory.
+int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem> &is,
+                      std::vector<pe::BatchItem> &iv)
+{
+    int max_mat = 1;
+    B->pair_nc4 = true;
+    for (PeSolver *S : B->solves)
+        if (S->pair_capable) {
+            max_mat = std::max(max_mat, S->cfg.n_mat);
+            B->pair_nc4 = B->pair_nc4 && S->cfg.n_coeffs == 4;
+        }
+    cudaFuncAttributes fa{};
+    PE_CUDA(cudaFuncGetAttributes(&fa, pe::k_stress_pair_batch<4, true>));
+    const size_t dyn_s = (size_t)optin - fa.sharedSizeBytes;
+    B->pair_ts = pe::PS_SMEM_FIXED + (size_t)max_mat * pe::TAB36 * sizeof(float) <= dyn_s;
+    B->smem_s = pe::PS_SMEM_FIXED + (B->pair_ts ? (size_t)max_mat * pe::TAB36 * sizeof(float) : 0);
+    B->smem_v = 128 + sizeof(float) * (3 * (size_t)pe::PV_SLOT + (size_t)max_mat);
+    PE_CUDA(cudaFuncGetAttributes(&fa, pe::k_velocity_pair_batch<4>));
+    if (B->smem_v > (size_t)optin - fa.sharedSizeBytes) return fail(PE_ERR_UNSUPPORTED, "density table too large");
+    auto setattr = [&](const void *f, size_t bytes) {
+        return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<4, true>, B->smem_s));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<4, false>, B->smem_s));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, true>, B->smem_s));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, false>, B->smem_s));
+    PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<4>, B->smem_v));
+    PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<0>, B->smem_v));
+    for (int s = 0; s < (int)B->solves.size(); ++s) {
+        PeSolver *S = B->solves[s];
+        if (!S->pair_capable) continue;
+        const PeConfig &c = S->cfg;
+        const int zc = S->zc_s;
+        const int nzc = (c.nz + zc - 1) / zc;
+        for (int bz = 0; bz < nzc; ++bz) {
+            for (int by = 0; by < (c.ny + pe::PS_OY - 1) / pe::PS_OY; ++by)
+                for (int bx = 0; bx < (c.nx + pe::PS_OX) / pe::PS_OX; ++bx) is.push_back({s, bx, by, bz});
+            for (int by = 0; by < (c.ny + pe::PV_OY - 1) / pe::PV_OY; ++by)
+                for (int bx = 0; bx < (c.nx + pe::PV_OX - 1) / pe::PV_OX; ++bx) iv.push_back({s, bx, by, bz});
+        }
+    }
+    B->grid_s = std::max(1, std::min((int)is.size(), nsm));
+    B->grid_v = std::max(1, std::min((int)iv.size(), nsm));
+    return PE_OK;
+}
 
 template <typename T>
 int batch_layout(PeBatch *B)
@@ -1022,6 +1079,23 @@ int batch_layout(PeBatch *B)
     PE_CUDA(cudaGetDevice(&dev));
     PE_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     PE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    B->pair_batch = false;
+    if constexpr (std::is_same<T, float>::value) {
+        bool any = false;
+        for (PeSolver *S : B->solves) any = any || S->pair_capable;
+        if (any) {
+            B->pair_batch = true;
+            int rc0 = batch_layout_pair(B, nsm, optin, is, iv);
+            if (rc0 == PE_ERR_UNSUPPORTED) {
+                B->pair_batch = false;
+                is.clear();
+                iv.clear();
+            } else if (rc0) {
+                return rc0;
+            }
+        }
+    }
+    if (!B->pair_batch) {
     B->smem_s = pe::stress_tma_smem<T>(max_mat);
     B->smem_v = pe::velocity_tma_smem<T>(max_mat);
     cudaFuncAttributes fa_s{}, fa_v{};
@@ -1050,10 +1124,11 @@ int batch_layout(PeBatch *B)
                 for (int bx = 0; bx < (c.nx + pe::TB_X - 1) / pe::TB_X; ++bx) iv.push_back({s, bx, by, bz});
         }
     }
+    B->grid_s = std::max(1, std::min((int)is.size(), nsm * std::max(1, per_s)));
+    B->grid_v = std::max(1, std::min((int)iv.size(), nsm * std::max(1, per_v)));
+    }
     B->n_items_s = (int)is.size();
     B->n_items_v = (int)iv.size();
-    B->grid_s = std::max(1, std::min(B->n_items_s, nsm * std::max(1, per_s)));
-    B->grid_v = std::max(1, std::min(B->n_items_v, nsm * std::max(1, per_v)));
     if (B->items_s) cudaFree(B->items_s);
     if (B->items_v) cudaFree(B->items_v);
     B->items_s = B->items_v = nullptr;
@@ -1079,11 +1154,14 @@ int batch_upload(PeBatch *B, const PeState *states, void *const *traces)
     std::vector<pe::StepArgs<T>> descs(n);
     std::vector<pe::TmapsStress> ms(n);
     std::vector<pe::TmapsVelocity> mv(n);
+    std::vector<pe::TmapsPairStress> pms(n);
+    std::vector<pe::TmapsPairVelocity> pmv(n);
+    std::vector<const float *> tabs(n, nullptr);
     for (int s = 0; s < n; ++s) {
         PeSolver *S = B->solves[s];
         int rc = ensure_maps(S, &states[s]);
         if (rc) return rc;
-        if (batched(B, S) && !S->tma)
+        if (batched(B, S) && !(B->pair_batch ? S->pair : S->tma))
             return fail(PE_ERR_UNSUPPORTED, "batched solves need 16-byte aligned state buffers");
         descs[s] = make_args<T>(S, &states[s], 0);
         descs[s].step = B->step;
@@ -1091,10 +1169,16 @@ int batch_upload(PeBatch *B, const PeState *states, void *const *traces)
         descs[s].zc = S->zc_s;
         ms[s] = S->ms;
         mv[s] = S->mv;
+        pms[s] = S->mps;
+        pmv[s] = S->mpv;
+        tabs[s] = S->tab36;
     }
     PE_CUDA(cudaMemcpy(B->descs, descs.data(), sizeof(pe::StepArgs<T>) * n, cudaMemcpyHostToDevice));
     PE_CUDA(cudaMemcpy(B->maps_s, ms.data(), sizeof(pe::TmapsStress) * n, cudaMemcpyHostToDevice));
     PE_CUDA(cudaMemcpy(B->maps_v, mv.data(), sizeof(pe::TmapsVelocity) * n, cudaMemcpyHostToDevice));
+    PE_CUDA(cudaMemcpy(B->pmaps_s, pms.data(), sizeof(pe::TmapsPairStress) * n, cudaMemcpyHostToDevice));
+    PE_CUDA(cudaMemcpy(B->pmaps_v, pmv.data(), sizeof(pe::TmapsPairVelocity) * n, cudaMemcpyHostToDevice));
+    PE_CUDA(cudaMemcpy(B->tabs, tabs.data(), sizeof(const float *) * n, cudaMemcpyHostToDevice));
     B->states.assign(states, states + n);
     B->traces.assign(traces, traces + n);
     B->uploaded = true;
@@ -1110,7 +1194,26 @@ int batch_chunk(PeBatch *B, int len)
 {
     const dim3 block(pe::TB_X, pe::TB_Y, 1);
     for (int k = 0; k < len; ++k) {
-        if (B->n_items_s > 0) {
+        if constexpr (std::is_same<T, float>::value) {
+            if (B->pair_batch && B->n_items_s > 0) {
+                const pe::StepArgs<float> *d = (const pe::StepArgs<float> *)B->descs;
+                const int ns = B->n_items_s, nv = B->n_items_v;
+                if (B->pair_nc4 && B->pair_ts)
+                    pe::k_stress_pair_batch<4, true><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                else if (B->pair_nc4)
+                    pe::k_stress_pair_batch<4, false><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                else if (B->pair_ts)
+                    pe::k_stress_pair_batch<0, true><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                else
+                    pe::k_stress_pair_batch<0, false><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                if (B->pair_nc4)
+                    pe::k_velocity_pair_batch<4><<<B->grid_v, pe::PR_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
+                else
+                    pe::k_velocity_pair_batch<0><<<B->grid_v, pe::PR_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
+                B->launches += 2;
+            }
+        }
+        if (!B->pair_batch && B->n_items_s > 0) {
             pe::k_stress_tma_batch<T><<<B->grid_s, block, B->smem_s, B->stream>>>(
                 (const pe::StepArgs<T> *)B->descs, B->maps_s, B->nmats, B->items_s, B->n_items_s, k);
             pe::k_velocity_tma_batch<T><<<B->grid_v, block, B->smem_v, B->stream>>>(
@@ -1215,6 +1318,9 @@ int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const Pe
     if ((rc = dev_alloc(&B->maps_s, sizeof(pe::TmapsStress) * n))) return rc;
     if ((rc = dev_alloc(&B->maps_v, sizeof(pe::TmapsVelocity) * n))) return rc;
     if ((rc = dev_alloc(&B->nmats, sizeof(int) * n))) return rc;
+    if ((rc = dev_alloc(&B->pmaps_s, sizeof(pe::TmapsPairStress) * n))) return rc;
+    if ((rc = dev_alloc(&B->pmaps_v, sizeof(pe::TmapsPairVelocity) * n))) return rc;
+    if ((rc = dev_alloc(&B->tabs, sizeof(const float *) * n))) return rc;
     std::vector<int> nm(n);
     for (int s = 0; s < n; ++s) nm[s] = cfgs[s].n_mat;
     PE_CUDA(cudaMemcpy(B->nmats, nm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));

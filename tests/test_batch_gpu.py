@@ -110,3 +110,24 @@ def test_batch_of_only_unaligned_rows():
     out = batch.forward_batch(probs, autotune=False)
     ref = O.run_oracle(oracle_prob(probs[0], record=probs[0]["record"], damped_record=True), fma_mode=1)
     assert np.array_equal(out[0], ref)
+
+
+def test_pair_batch_large_table_and_mixed_orders():
+    """An FP32 batch whose largest table exceeds shared memory and whose
+    solves mix stencil orders (the pair kernels' general instantiations)."""
+    from pefdtd import batch
+    from pefdtd.coeffs import optimised_coeffs
+    a = dict(make_small(nt=60, shape=(14, 40, 40), n_grains=600, sponge=2, seed=21))
+    b6 = dict(make_small(nt=60, shape=(16, 36, 44), n_grains=7, sponge=2, seed=22))
+    b6["coeffs"] = optimised_coeffs(6)
+    probs = [a, b6]
+    bs = batch.BatchSolver([batch.spec_from_problem(p) for p in probs], z_chunk=5, chunk_steps=25)
+    try:
+        bs.run(0, 60)
+        got = bs.traces_numpy(60)
+    finally:
+        bs.close()
+    for p, tr in zip(probs, got):
+        ref = O.run_oracle(oracle_prob(p, record=p["record"], damped_record=True), fma_mode=1)
+        assert np.abs(ref).max() > 0
+        assert np.array_equal(tr, ref)
