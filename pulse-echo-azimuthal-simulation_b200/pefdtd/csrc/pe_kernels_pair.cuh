@@ -41,10 +41,21 @@ constexpr int PS_SW = 36, PS_SH = 30, PS_SSZ = PS_SW * PS_SH;     // cell box: 1
 constexpr int PS_SSZP = 1088;                                     // ... padded to 128 B
 constexpr int PS_GW = 32, PS_GOFF = 8, PS_GST = 1040;             // strain plane: pad, 32 x 32, pad
 constexpr int PS_VSLOT = 3 * PS_VSZ;
-constexpr int PS_SSLOT = 7 * PS_SSZP;
+constexpr int PS_SSLOT = 6 * PS_SSZP;
+// Strain ring: the update of plane z reads g4 and g5 at planes z - 1 and z,
+// the other four components at z and z + 1 (the half-cell moves,
+// sim/core/fdtd.py:612-633). While it runs, the strains of plane z + 2 are
+// written; with four planes for g4, g5 and three for the others they never
+// overwrite what the update reads, so one block barrier per plane suffices.
+__host__ __device__ constexpr int ring_planes(int J) { return (J == 3 || J == 4) ? 4 : 3; }
+__host__ __device__ constexpr int ring_base(int J)   // first plane of component J, in planes
+{
+    return J < 3 ? 3 * J : (J == 5 ? 9 : (J == 3 ? 12 : 16));
+}
+constexpr int PS_RING = 20;   // strain planes held
 // shared memory of a stress block: mbarriers (v, cell slot 0, cell slot 1),
-// one v slot, two cell slots, three strain planes, then the material table
-constexpr size_t PS_SMEM_FIXED = 128 + sizeof(float) * ((size_t)PS_VSLOT + 2 * (size_t)PS_SSLOT + (size_t)3 * 6 * PS_GST);
+// one v slot, two cell slots, the strain ring, then the material table
+constexpr size_t PS_SMEM_FIXED = 128 + sizeof(float) * ((size_t)PS_VSLOT + 2 * (size_t)PS_SSLOT + (size_t)PS_RING * PS_GST);
 constexpr int TAB36 = 36;   // material: columns J as [C0J..C3J] at 4J, then [C4J, C5J] at 24 + 2J
 // velocity
 constexpr int PV_OX = 32, PV_OY = 32;
@@ -164,11 +175,14 @@ __device__ __forceinline__ void pair_strain(const StepArgs<float> &A, int q, con
     }
 }
 
-// strain J at (dz, dy) and column offset dx in -1..2 from cell 0; pl[k] is
-// the ring plane of dz = k - 1 at this thread's cell 0
-__device__ __forceinline__ float gval(const float *const (&pl)[3], int J, int dz, int dy, int dx)
+// strain J at (dz, dy) and column offset dx in -1..2 from cell 0. pl[0]:
+// the 4-plane ring slot of plane z - 1, pl[1] of z (both at this thread's
+// cell 0, component offsets added here); pl[2]: the 3-plane ring slot of
+// z, pl[3] of z + 1.
+__device__ __forceinline__ float gval(const float *const (&pl)[4], int J, int dz, int dy, int dx)
 {
-    const float *p = pl[dz + 1] + J * PS_GST + dy * PS_GW + (dx & ~1);
+    const float *b = (J == 3 || J == 4) ? pl[dz + 1] : pl[dz + 2];
+    const float *p = b + ring_base(J) * PS_GST + dy * PS_GW + (dx & ~1);
     const float2 v = lds2(p);
     return (dx & 1) ? v.y : v.x;
 }
@@ -181,7 +195,7 @@ struct MoveGuards {
 // 4 taps summed z-major, times 1/4, zero where a needed neighbour is off
 // the grid; the term order of qval() in pe_kernels.cuh
 template <int P, int J, bool G>
-__device__ __forceinline__ void qpair(const float *const (&pl)[3], const MoveGuards &mg, float (&q)[2])
+__device__ __forceinline__ void qpair(const float *const (&pl)[4], const MoveGuards &mg, float (&q)[2])
 {
     constexpr int S = vpos(J);
     constexpr int DZ = pos_z(P) - pos_z(S), DY = pos_y(P) - pos_y(S), DX = pos_x(P) - pos_x(S);
@@ -225,7 +239,7 @@ __device__ __forceinline__ void qpair(const float *const (&pl)[3], const MoveGua
 // the position of stress I), J ascending as in row_dot(). TS: the table is
 // in shared memory (else global, through the read-only cache).
 template <int J, bool G, bool TS>
-__device__ __forceinline__ void stiff_column(const float *const (&pl)[3], const MoveGuards &mg,
+__device__ __forceinline__ void stiff_column(const float *const (&pl)[4], const MoveGuards &mg,
                                              const float *const (&crow)[2], float (&acc)[6][2])
 {
     float q0[2], q1[2], q2[2], q3[2];
@@ -247,7 +261,7 @@ __device__ __forceinline__ void stiff_column(const float *const (&pl)[3], const 
 }
 
 template <bool G, bool TS>
-__device__ __forceinline__ void stiff_all(const float *const (&pl)[3], const MoveGuards &mg,
+__device__ __forceinline__ void stiff_all(const float *const (&pl)[4], const MoveGuards &mg,
                                           const float *const (&crow)[2], float (&acc)[6][2])
 {
 #pragma unroll
@@ -268,11 +282,12 @@ struct PairPhases {
 // One z-march of a block over strain tile (bx, by), updating planes
 // [zb, ze). tab: the (n_mat, 36) table (shared memory when TS). Pipeline per
 // iteration (strain plane q, update plane z = q - 1):
-//   wait v(q) | sync A | issue cell box z + 1 | strains of q | wait cell box z
-//   | sync B | issue v(q + 1) | updates of plane z
-// One v slot suffices (its refill overlaps the update phase); the cell boxes
-// alternate between two slots and are issued a plane ahead. The caller
-// synchronises the block before a march that follows another.
+//   wait v(q) | strains of q | block barrier | issue v(q + 1) and the cell
+//   boxes of z + 1 | wait cell boxes of z | updates of plane z
+// Every warp waits on the mbarriers itself. One v slot suffices (its refill
+// overlaps the update phase); the cell boxes alternate between two slots and
+// are issued a plane ahead. The caller synchronises the block before a march
+// that follows another.
 template <int NC, bool TS>
 __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, const StepArgs<float> &A,
                                                   const float *tab, unsigned char *smem, int bx, int by,
@@ -283,6 +298,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     float *sslots = vslot + PS_VSLOT;
     float *gs = sslots + 2 * PS_SSLOT;
     const int tid = threadIdx.x;
+    (void)tab;
     const int l = tid & (PR_LX - 1), r = tid >> 4;
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const long long sy = A.sy, sz = A.sz;
@@ -295,7 +311,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     const int xv = floor4(S0 - T_H), xs = floor4(S0);    // box x-origins (16-byte multiples)
     const int q0 = zb - 1;
     const bool has_dvol = A.dvol != nullptr;
-    const unsigned bytes_s = (6u * PS_SSZ + (has_dvol ? (unsigned)PS_SSZ : 0u)) * 4u;
+    const unsigned bytes_s = 6u * PS_SSZ * 4u;
     const unsigned bytes_v = 3u * PS_VSZ * 4u;
     const int v0 = ph.v, s0 = ph.s;   // phase counts at the start of this march
 
@@ -313,7 +329,6 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         mbar_expect_tx(bar, bytes_s);
 #pragma unroll
         for (int f = 0; f < 6; ++f) tma_load_3d(ds + f * PS_SSZP, &M.sc[f], xs, S0y + 1, z, bar);
-        if (has_dvol) tma_load_3d(ds + 6 * PS_SSZP, &M.dv, xs, S0y + 1, z, bar);
     };
 
     // z rings (rz[c][k] <-> plane q-4+k, ry/rx[c][k] <-> q-3+k), one plane ahead
@@ -375,10 +390,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     const int n_it = ze - q0 + 1;
     for (int i = 0; i < n_it; ++i) {
         const int q = q0 + i;
-        const int sl = i % 3;   // strain ring slot of plane q
-        if (tid < 32) mbar_wait(bars, (unsigned)(v0 + i) & 1u, status);
-        __syncthreads();   // A: v(q) landed (observed by warp 0); the updates of plane q - 2 are done
-        if (tid == 0 && q >= zb + 2 && q < ze) issue_s(q);   // into the slot plane q - 2 used
+        mbar_wait(bars, (unsigned)(v0 + i) & 1u, status);   // v(q) landed
         const float2 nzv = ld2col(pz, q + 4), nyv = ld2col(py, q + 5), nxv = ld2col(px, q + 5);
         const int z = q - 1;
         const uint32_t lab2 = lab_next;
@@ -389,9 +401,10 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
             float g[2][6];
             if (fast) pair_strain<NC, false>(A, q, tv, rz, ry, rx, tl, g);
             else pair_strain<NC, true>(A, q, tv, rz, ry, rx, tl, g);
-            float *gw = gs + sl * 6 * PS_GST + cg;
+            const int s3 = (q + 12) % 3, s4 = (q + 12) % 4;   // ring slots of plane q (q >= -1)
 #pragma unroll
-            for (int J = 0; J < 6; ++J) stg2(gw + J * PS_GST, g[0][J], g[1][J]);
+            for (int J = 0; J < 6; ++J)
+                stg2(gs + (ring_base(J) + (ring_planes(J) == 4 ? s4 : s3)) * PS_GST + cg, g[0][J], g[1][J]);
         }
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
@@ -405,15 +418,17 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         rz[0][7] = nzv.x; rz[1][7] = nzv.y;
         ry[0][7] = nyv.x; ry[1][7] = nyv.y;
         rx[0][7] = nxv.x; rx[1][7] = nxv.y;
+        __syncthreads();   // strains of q written; the v slot is free; the updates of z - 1 are done
+        if (tid == 0) {
+            if (q + 1 <= ze) issue_v(q + 1);
+            if (q >= zb + 2 && q < ze) issue_s(q);   // plane z + 1, into the slot plane z - 1 used
+        }
         const int us = s0 + z - zb;   // cell-box load index of plane z
-        if (tid < 32 && z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
-        __syncthreads();   // B: strains of q written; the v slot is free; cell box z landed
-        if (tid == 0 && q + 1 <= ze) issue_v(q + 1);
+        if (z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
         if (z >= zb && any_out) {
-            // strain planes z-1, z, z+1 were written at iterations i-2, i-1, i
-            const float *const pl[3] = {gs + ((i + 1) % 3) * 6 * PS_GST + cg,
-                                        gs + ((i + 2) % 3) * 6 * PS_GST + cg,
-                                        gs + sl * 6 * PS_GST + cg};
+            // strain planes z - 1, z, z + 1 were written at iterations i - 2, i - 1, i
+            const float *const pl[4] = {gs + ((z + 11) % 4) * PS_GST + cg, gs + ((z + 12) % 4) * PS_GST + cg,
+                                        gs + ((z + 12) % 3) * PS_GST + cg, gs + ((z + 13) % 3) * PS_GST + cg};
             mg.zlo = z >= 1;
             mg.zhi = z <= nz - 2;
             const uint16_t lab[2] = {(uint16_t)(lab2 & 0xFFFFu), (uint16_t)(lab2 >> 16)};
@@ -426,7 +441,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
             {
                 const float dz = A.dz ? A.dz[z] : 1.0f;
                 float2 dvv = make_float2(1.0f, 1.0f);
-                if (has_dvol) dvv = lds2(sc + 6 * PS_SSZP);
+                if (has_dvol) dvv = ldg2(A.dvol + (long long)z * sz + col);
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
                     float d = 1.0f;
@@ -505,7 +520,7 @@ __device__ __forceinline__ void stress_pair_init(unsigned char *smem)
         fence_mbar_init();
     }
     // zero the strain planes' pads (read only by cells that are not updated)
-    for (int i = threadIdx.x; i < 3 * 6 * 2 * PS_GOFF; i += blockDim.x) {
+    for (int i = threadIdx.x; i < PS_RING * 2 * PS_GOFF; i += blockDim.x) {
         const int p = i / (2 * PS_GOFF), k = i % (2 * PS_GOFF);
         gs[p * PS_GST + (k < PS_GOFF ? k : PS_GST - 2 * PS_GOFF + k)] = 0.f;
     }
