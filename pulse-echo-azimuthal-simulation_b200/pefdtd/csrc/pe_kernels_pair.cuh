@@ -388,6 +388,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         if (zb + 1 < ze) issue_s(zb + 1);
     }
     const int n_it = ze - q0 + 1;
+    int r3 = (q0 + 3) % 3;   // plane q modulo 3 (q >= -1), kept by increment
     for (int i = 0; i < n_it; ++i) {
         const int q = q0 + i;
         mbar_wait(bars, (unsigned)(v0 + i) & 1u, status);   // v(q) landed
@@ -401,10 +402,10 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
             float g[2][6];
             if (fast) pair_strain<NC, false>(A, q, tv, rz, ry, rx, tl, g);
             else pair_strain<NC, true>(A, q, tv, rz, ry, rx, tl, g);
-            const int s3 = (q + 12) % 3, s4 = (q + 12) % 4;   // ring slots of plane q (q >= -1)
+            const int s4 = q & 3;   // ring slots of plane q: r3 and q mod 4
 #pragma unroll
             for (int J = 0; J < 6; ++J)
-                stg2(gs + (ring_base(J) + (ring_planes(J) == 4 ? s4 : s3)) * PS_GST + cg, g[0][J], g[1][J]);
+                stg2(gs + (ring_base(J) + (ring_planes(J) == 4 ? s4 : r3)) * PS_GST + cg, g[0][J], g[1][J]);
         }
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
@@ -427,8 +428,9 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         if (z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
         if (z >= zb && any_out) {
             // strain planes z - 1, z, z + 1 were written at iterations i - 2, i - 1, i
-            const float *const pl[4] = {gs + ((z + 11) % 4) * PS_GST + cg, gs + ((z + 12) % 4) * PS_GST + cg,
-                                        gs + ((z + 12) % 3) * PS_GST + cg, gs + ((z + 13) % 3) * PS_GST + cg};
+            const int zr3 = r3 == 0 ? 2 : r3 - 1;   // plane z modulo 3
+            const float *const pl[4] = {gs + ((z - 1) & 3) * PS_GST + cg, gs + (z & 3) * PS_GST + cg,
+                                        gs + zr3 * PS_GST + cg, gs + r3 * PS_GST + cg};
             mg.zlo = z >= 1;
             mg.zhi = z <= nz - 2;
             const uint16_t lab[2] = {(uint16_t)(lab2 & 0xFFFFu), (uint16_t)(lab2 >> 16)};
@@ -498,6 +500,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
                 }
             }
         }
+        r3 = r3 == 2 ? 0 : r3 + 1;
     }
     ph.v = v0 + n_it;
     ph.s = s0 + (ze - zb);
