@@ -20,6 +20,13 @@ slowest rank's device time.
 --impl reference runs the reference's own update kernels, compiled for the
 host CPU from the reference sources (oracle/_ref; oracle port if absent), on
 all host cores, rank 0 only, time-boxed.
+
+--sweep N prints one line comparing an N-solve sweep of the workload grid
+run batched (one launch pair per step for all solves, pefdtd.batch) against
+the plain loop (one solve at a time, each created, run and read back in
+turn); both timings include solver set-up and trace download. --uneven adds
+24 solves of uneven grids (128 x 128 x 96 ... 256 x 256 x 160, 100-800
+grains, Watson kappa 0-20) to the batch.
 """
 from __future__ import annotations
 
@@ -204,6 +211,74 @@ def _cpu_run(p, budget_s, max_steps):
     return ncell * n / el / 1e9, n, cores, kind, sample
 
 
+def _uneven_specs(n=24):
+    """Uneven disks: grids from 128 x 128 x 96 to 256 x 256 x 160 (rows of
+    16-byte multiples), 100-800 grains, Watson kappa 0-20, seeded."""
+    out = []
+    for i in range(n):
+        f = i / max(1, n - 1)
+        nxy = int(round((128 + 128 * f) / 16)) * 16
+        nz = int(round((96 + 64 * f) / 8)) * 8
+        h = 0.1e-3
+        d = (nxy - 70) * h
+        out.append(dict(shape=(nz, nxy, nxy), h=h, diameter=d, height=min(10e-3, (nz - 70) * h),
+                        n_grains=int(100 + 700 * ((i * 7) % n) / max(1, n - 1)),
+                        fabric=("watson", 30.0, 20.0 * ((i * 5) % n) / max(1, n - 1)),
+                        f0=2.25e6, n_cycles=5, nt=6000, sponge=32, aperture=6e-3, seed=100 + i))
+    return out
+
+
+def _sweep(args):
+    """Batched vs plain N-solve sweep (one line of JSON)."""
+    import torch
+    from pefdtd import batch, workloads
+    from pefdtd.fdtd import _flat_probe
+    from pefdtd.damping import sponge_axis_profiles
+    K = int(args.steps)
+    base = workloads.make_problem(args.workload, nt=K + 8)
+    probs = [base] * int(args.sweep)
+    if args.uneven:
+        probs = probs + [workloads.make_problem(sp, nt=K + 8) for sp in _uneven_specs()]
+    cells = sum(int(np.prod(p["lab"].shape)) for p in probs)
+    specs = [batch.spec_from_problem(p) for p in probs]
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = []
+    for p in probs:
+        shape = p["lab"].shape
+        s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float32)
+        from pefdtd.fdtd import DeviceSolve
+        sv = DeviceSolve(p["mats"], p["Ct"], p["rho_t"], p["h"], p["dt"], p["coeffs"], s_idx, s_w,
+                         r_off, r_idx, r_w, record=p["record"], damped_record=True,
+                         sponge=sponge_axis_profiles(shape, p["sponge"]))
+        sv.set_wavelet(p["wavelet"][:K])
+        sv.run(0, K)
+        plain.append(sv.traces_numpy(K))
+        sv.close()
+        del sv
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    b = batch.BatchSolver(specs)
+    try:
+        b.run(0, K)
+        got = b.traces_numpy(K)
+    finally:
+        b.close()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    same = all(np.array_equal(a, g[:K]) for a, g in zip(plain, got))
+    return {"metric": "sweep Gcell-updates/s, batched vs plain loop", "unit": "Gcell-updates/s",
+            "solves": len(probs), "steps": K, "cells_per_step": cells,
+            "plain": cells * K / t_plain / 1e9, "batched": cells * K / t_batch / 1e9,
+            "speedup": t_plain / t_batch, "plain_s": t_plain, "batched_s": t_batch,
+            "traces_identical": bool(same),
+            "config": {"workload": args.workload, "uneven24": bool(args.uneven),
+                       "timing": "wall clock, set-up and trace download included, synchronised"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -213,6 +288,8 @@ def main():
     ap.add_argument("--workload", default="disk_prod")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sweep", type=int, default=0)
+    ap.add_argument("--uneven", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -235,6 +312,11 @@ def main():
                 "e2e": {"value": val, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+
+    if args.sweep:
+        if rank == 0:
+            print(json.dumps(_sweep(args)), flush=True)
         return
 
     import torch
