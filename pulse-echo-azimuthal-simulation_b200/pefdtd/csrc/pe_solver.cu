@@ -105,6 +105,7 @@ struct PeSolver {
     float *tab36 = nullptr;     // (n_mat, 36) column-split stiffness
     bool pair_capable = false;  // FP32, rows of 16-byte multiples, maps encodable, smem fits
     bool pair = false;          // pair kernels in use for the current state
+    bool solo = false;          // in a batch: fills the GPU alone, so runs its own launches
     int zc_ps = 0, zc_pv = 0;   // planes per z-march of the pair launches
     pe::TmapsPairStress mps{};
     pe::TmapsPairVelocity mpv{};
@@ -398,12 +399,14 @@ int configure_kernels(PeSolver *S)
         S->pair_capable = S->variant == PE_KERNEL_TILED && c.nx % 4 == 0 && ps <= (size_t)optin &&
                           pv <= (size_t)optin && encode_fn() != nullptr;
         if (S->pair_capable) {
-            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-            PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pv));
-            PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pv));
+            // the attribute belongs to the kernel, not to this solve: allow the
+            // device maximum so that solves with other table sizes can coexist
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_stress_pair<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             const long long tps = (long long)((c.nx + pe::PS_OX) / pe::PS_OX) * ((c.ny + pe::PS_OY - 1) / pe::PS_OY);
             const long long tpv = (long long)((c.nx + pe::PV_OX - 1) / pe::PV_OX) * ((c.ny + pe::PV_OY - 1) / pe::PV_OY);
             const int sps = occupancy_slots(pe::k_stress_pair<4, true>, pe::PR_N, ps);
@@ -1012,7 +1015,7 @@ namespace {
 // Whether solve S runs inside the batched TMA launches (else its own pair).
 bool batched(const PeBatch *B, const PeSolver *S)
 {
-    return B->pair_batch ? S->pair_capable : (B->tma_batch && S->tma_capable);
+    return B->pair_batch ? (S->pair_capable && !S->solo) : (B->tma_batch && S->tma_capable);
 }
 
 // Pair-kernel layout of an FP32 batch: work items, grids and shared memory.
@@ -1021,11 +1024,19 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
 {
     int max_mat = 1;
     B->pair_nc4 = true;
-    for (PeSolver *S : B->solves)
-        if (S->pair_capable) {
+    // a solve whose own launches fill every SM at least twice runs them
+    // inside the batch's graph; the shared persistent launches are for the
+    // solves too small to fill the GPU alone
+    for (PeSolver *S : B->solves) {
+        const PeConfig &c = S->cfg;
+        const long long tiles = (long long)((c.nx + pe::PS_OX) / pe::PS_OX) * ((c.ny + pe::PS_OY - 1) / pe::PS_OY);
+        const long long blocks = tiles * ((c.nz + S->zc_ps - 1) / std::max(1, S->zc_ps));
+        S->solo = S->pair_capable && S->zc_ps > 0 && blocks >= 2LL * nsm;
+        if (S->pair_capable && !S->solo) {
             max_mat = std::max(max_mat, S->cfg.n_mat);
             B->pair_nc4 = B->pair_nc4 && S->cfg.n_coeffs == 4;
         }
+    }
     cudaFuncAttributes fa{};
     PE_CUDA(cudaFuncGetAttributes(&fa, pe::k_stress_pair_batch<4, true>));
     const size_t dyn_s = (size_t)optin - fa.sharedSizeBytes;
@@ -1034,18 +1045,22 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
     B->smem_v = 128 + sizeof(float) * (3 * (size_t)pe::PV_SLOT + (size_t)max_mat);
     PE_CUDA(cudaFuncGetAttributes(&fa, pe::k_velocity_pair_batch<4>));
     if (B->smem_v > (size_t)optin - fa.sharedSizeBytes) return fail(PE_ERR_UNSUPPORTED, "density table too large");
-    auto setattr = [&](const void *f, size_t bytes) {
-        return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // per-kernel attributes: the largest dynamic size any batch may use
+    auto setattr = [&](const void *f) {
+        cudaFuncAttributes a{};
+        cudaError_t e = cudaFuncGetAttributes(&a, f);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
     };
-    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<4, true>, B->smem_s));
-    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<4, false>, B->smem_s));
-    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, true>, B->smem_s));
-    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, false>, B->smem_s));
-    PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<4>, B->smem_v));
-    PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<0>, B->smem_v));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<4, true>));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<4, false>));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, true>));
+    PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, false>));
+    PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<4>));
+    PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<0>));
     for (int s = 0; s < (int)B->solves.size(); ++s) {
         PeSolver *S = B->solves[s];
-        if (!S->pair_capable) continue;
+        if (!batched(B, S)) continue;
         const PeConfig &c = S->cfg;
         const int zc = S->zc_s;
         const int nzc = (c.nz + zc - 1) / zc;

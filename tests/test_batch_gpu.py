@@ -131,3 +131,24 @@ def test_pair_batch_large_table_and_mixed_orders():
         ref = O.run_oracle(oracle_prob(p, record=p["record"], damped_record=True), fma_mode=1)
         assert np.abs(ref).max() > 0
         assert np.array_equal(tr, ref)
+
+
+def test_batch_mixing_solo_and_shared_solves():
+    """A solve large enough to fill the GPU alone runs its own launches inside
+    the batch's graph next to small solves in the shared launches; tables of
+    different sizes coexist (kernel attributes are per kernel, not per solve)."""
+    from pefdtd import batch
+    big = make_small(nt=40, shape=(40, 256, 256), n_grains=300, sponge=4, seed=31)
+    small = [make_small(nt=40, shape=(20, 28, 32), n_grains=5, sponge=3, seed=32),
+             make_small(nt=40, shape=(18, 36, 40), n_grains=40, sponge=3, seed=33)]
+    probs = [big] + small
+    b = batch.BatchSolver([batch.spec_from_problem(p) for p in probs], chunk_steps=20)
+    try:
+        b.run(0, 40)
+        got = b.traces_numpy(40)
+    finally:
+        b.close()
+    for p, tr in zip(probs, got):
+        ref = O.run_oracle(oracle_prob(p, record=p["record"], damped_record=True), fma_mode=1)
+        assert np.abs(ref).max() > 0
+        assert np.array_equal(tr, ref)
