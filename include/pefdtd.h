@@ -231,6 +231,18 @@ int pe_label_cylinder(const double *xs, int nx, const double *ys, int ny, const 
                       int nz, double R2, const double *seeds, const double *weights, int ns,
                       int32_t *out_dev, void *stream);
 
+/* Solver grid of a specimen rotated by -rot about z (azimuth sweep; replaces
+ * the reference's rotated_grid, sim/core/rotation_test.py:60-137, with its
+ * nearest resample by np.rint). labels_dev: device int32 (nx_s, nx_s, nz_s)
+ * specimen labels (x, y, z order, -1 outside) at spacing h_spec. out_dev:
+ * device int32 (ndz + 2m, nd + 2m, nd + 2m) solver labels (z, y, x), -1 in
+ * the padding and where the rotated sample leaves the specimen; nd and ndz
+ * the core extents (round(nx_s*h_spec/h), round(nz_s*h_spec/h)), m the
+ * padding (sponge + 3), cos_a / sin_a of the rotation angle. Bit-identical
+ * to the host computation. Synchronous on `stream`. */
+int pe_rotated_grid(const int32_t *labels_dev, int nx_s, int nz_s, double h_spec, double h, int nd,
+                    int ndz, double cos_a, double sin_a, int m, int32_t *out_dev, void *stream);
+
 /* Allocation-free variant of pe_label_cylinder, with no counterpart in the
  * reference. For callers that may not allocate device memory (an application
  * whose framework has reserved the device pool for its own allocator, or a

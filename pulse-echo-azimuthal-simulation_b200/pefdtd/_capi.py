@@ -94,6 +94,8 @@ def lib():
         L.pe_label_cylinder.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                         C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_void_p]
+        L.pe_rotated_grid.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                      C.c_int, C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         if L.pe_abi_version() != ABI_VERSION:
             raise RuntimeError("pefdtd library ABI mismatch; rebuild with pefdtd.build")
         _lib = L
@@ -121,6 +123,6 @@ def exported_symbols():
     return ["pe_abi_version", "pe_last_error", "pe_solver_create", "pe_solver_set_wavelet",
             "pe_solver_run", "pe_solver_launch_count", "pe_solver_profile", "pe_solver_status",
             "pe_solver_destroy",
-            "pe_forward_host", "pe_label_cylinder", "pe_batch_create", "pe_batch_schedule",
+            "pe_forward_host", "pe_label_cylinder", "pe_rotated_grid", "pe_batch_create", "pe_batch_schedule",
             "pe_batch_set_wavelet", "pe_batch_run", "pe_batch_status", "pe_batch_launch_count",
             "pe_batch_destroy"]

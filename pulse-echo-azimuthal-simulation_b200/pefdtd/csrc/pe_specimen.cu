@@ -63,9 +63,66 @@ __global__ void k_label_cylinder(const double *__restrict__ xs, const double *__
     if (live) out[i] = inside ? arg : -1;
 }
 
+// Solver grid of a specimen rotated by -rot about z, resampled by nearest
+// neighbour (reference sim/core/rotation_test.py:60-137, restated in
+// pefdtd/specimen.py rotated_grid): the core cell (k, j, i) samples the
+// specimen label at
+//   gi = rint((ca*u_i - sa*u_j) / h_spec + c),  gj = rint((sa*u_i + ca*u_j) / h_spec + c),
+//   gz = trunc(clip(((k + 0.5)*h) / h_spec, 0, nz_s - 1)),
+// u_i = (i + 0.5)*h - D/2, c = (nx_s - 1)/2, or -1 where (gi, gj) leaves
+// the specimen; every expression in the NumPy evaluation order, float64,
+// no fused multiply-add (-fmad=false), rint rounding half to even as
+// np.rint. The core sits at offset m in each axis of the output, whose
+// other cells the host fills with -1.
+__global__ void k_rotated_grid(const int32_t *__restrict__ lab_xyz, int nx_s, int nz_s, int nd, int ndz,
+                               double h, double h_spec, double half_d, double ca, double sa, double c_off,
+                               int m, int nxo, int32_t *__restrict__ out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)nd * nd * ndz;
+    if (t >= n) return;
+    const int i = (int)(t % nd);
+    const int j = (int)((t / nd) % nd);
+    const int k = (int)(t / ((long long)nd * nd));
+    const double ui = ((double)i + 0.5) * h - half_d;
+    const double uj = ((double)j + 0.5) * h - half_d;
+    const double xr = ca * ui - sa * uj;
+    const double yr = sa * ui + ca * uj;
+    const long long gi = (long long)rint(xr / h_spec + c_off);
+    const long long gj = (long long)rint(yr / h_spec + c_off);
+    double tz = ((double)k + 0.5) * h / h_spec;
+    tz = fmin(fmax(tz, 0.0), (double)(nz_s - 1));
+    const int gz = (int)tz;
+    int32_t v = -1;
+    if (gi >= 0 && gi < nx_s && gj >= 0 && gj < nx_s) v = lab_xyz[(gi * nx_s + gj) * nz_s + gz];
+    out[((long long)(m + k) * nxo + (m + j)) * nxo + (m + i)] = v;
+}
+
 thread_local std::string g_err_spec;
 
 }  // namespace
+
+extern "C" int pe_rotated_grid(const int32_t *labels_dev, int nx_s, int nz_s, double h_spec, double h,
+                               int nd, int ndz, double cos_a, double sin_a, int m, int32_t *out_dev,
+                               void *stream)
+{
+    if (!labels_dev || !out_dev || nx_s < 1 || nz_s < 1 || nd < 1 || ndz < 1 || m < 0 || !(h > 0) ||
+        !(h_spec > 0))
+        return PE_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long nxo = nd + 2LL * m, nzo = ndz + 2LL * m;
+    cudaError_t e = cudaMemsetAsync(out_dev, 0xFF, sizeof(int32_t) * (size_t)(nzo * nxo * nxo), st);
+    if (e == cudaSuccess) {
+        const double D = nx_s * h_spec;
+        const long long n = (long long)nd * nd * ndz;
+        k_rotated_grid<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(labels_dev, nx_s, nz_s, nd, ndz, h, h_spec,
+                                                                   D / 2.0, cos_a, sin_a, (nx_s - 1) / 2.0, m,
+                                                                   (int)nxo, out_dev);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+}
 
 extern "C" int pe_label_cylinder(const double *xs, int nx, const double *ys, int ny,
                                  const double *zs, int nz, double R2, const double *seeds,

@@ -364,6 +364,35 @@ def build_grid(labels_xyz, h_spec, h, sponge):
     return lab, nd, m
 
 
+def rotated_grid_device(labels_xyz, axes, h_spec, h, sponge, rot_deg, device=None):
+    """rotated_grid on the GPU (pe_rotated_grid): the same (lab, nd, m,
+    axes_rot), bit for bit, with lab a device int32 tensor. labels_xyz: the
+    specimen labels (x, y, z), numpy or a device tensor."""
+    from . import _capi
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("rotated_grid_device runs on a CUDA device; use rotated_grid on CPU")
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if isinstance(labels_xyz, torch.Tensor):
+        lab_in = labels_xyz.to(device=dev, dtype=torch.int32).contiguous()
+    else:
+        lab_in = torch.from_numpy(np.ascontiguousarray(labels_xyz, np.int32)).to(dev)
+    nx_s, _, nz_s = lab_in.shape
+    D = nx_s * h_spec
+    nd = int(round(D / h))
+    ndz = int(round(nz_s * h_spec / h))
+    a = np.radians(rot_deg)
+    ca, sa = np.cos(a), np.sin(a)
+    m = sponge + 3
+    out = torch.empty((ndz + 2 * m, nd + 2 * m, nd + 2 * m), dtype=torch.int32, device=dev)
+    with torch.cuda.device(dev):
+        _capi.check(_capi.lib().pe_rotated_grid(
+            lab_in.data_ptr(), nx_s, nz_s, float(h_spec), float(h), nd, ndz, float(ca), float(sa), m,
+            out.data_ptr(), _capi.C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    R = np.array([[ca, -sa, 0.0], [sa, ca, 0.0], [0.0, 0.0, 1.0]])
+    return out, nd, m, np.asarray(axes, float) @ R
+
+
 def rotated_grid(labels_xyz, axes, h_spec, h, sponge, rot_deg):
     """Solver grid of the specimen rotated by -rot_deg about z (nearest
     resample with np.rint), with the c-axes rotated the same way

@@ -242,6 +242,12 @@ def azimuth_setup(cfg, build, co, az, labeller=None):
     if cfg.get("rasterise") == "single":
         lab, nd, _, axes_rot = specimen.rotated_grid_single_raster(build, h, cfg["sponge"], az,
                                                                    labeller=labeller)
+    elif specimen.pick_labeller(labeller=labeller) == "gpu":
+        # the same resample on the device (bit-identical), read back for the
+        # host-side probe, damping mask and time step
+        lab_d, nd, _, axes_rot = specimen.rotated_grid_device(build["labels"], build["axes"], build["h"],
+                                                              h, cfg["sponge"], az)
+        lab = lab_d.cpu().numpy()
     else:
         lab, nd, _, axes_rot = specimen.rotated_grid(build["labels"], build["axes"], build["h"], h,
                                                      cfg["sponge"], az)
