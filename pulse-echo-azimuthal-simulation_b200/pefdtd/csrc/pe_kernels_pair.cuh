@@ -372,6 +372,9 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     }
     const bool tile_in = S0 - T_H >= 0 && S0 + PS_GW - 1 + T_H < nx && S0y - T_H >= 0 &&
                          S0y + PR_ROWS - 1 + T_H < ny;
+    // a warp's two rows both past the last grid row: no strain of theirs is
+    // read by an updated cell, so the warp skips the strain work (warp-uniform)
+    const bool warp_rows_in = S0y + 2 * (tid >> 5) < ny;
     const int cv = (r + T_H) * PS_VW + (S0 - xv) + 2 * l;   // cell 0 in a v box (even)
     const int cs = (r - 1) * PS_SW + (S0 - xs) + 2 * l;     // cell 0 in a cell box (even)
     const int cg = PS_GOFF + r * PS_GW + 2 * l;              // cell 0 in a strain plane
@@ -397,7 +400,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         const uint32_t lab2 = lab_next;
         lab_next = ldlab(q);
         const bool fast = NC == 4 && tile_in && q >= T_H && q <= nz - 1 - T_H;
-        {
+        if (warp_rows_in) {
             const float *tv = vslot + cv;
             float g[2][6];
             if (fast) pair_strain<NC, false>(A, q, tv, rz, ry, rx, tl, g);
