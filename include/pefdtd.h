@@ -193,6 +193,19 @@ typedef struct PeAdjoint {
 int pe_solver_adjoint_step(PeSolver *s, const PeAdjoint *adj, int64_t n, const void *residual,
                            void *stream);
 
+/* One checkpoint segment of the reverse sweep in a single call: `state`
+ * holds the forward state before step `step_begin` (restored from its
+ * checkpoint by the caller); the call recomputes steps [step_begin,
+ * step_end) forward on `state`, keeping v before each step in `v_hist`
+ * (device, (step_end - step_begin, 3, nz, ny, nx) of dtype), then applies
+ * pe_solver_adjoint_step for n = step_end - 1 down to step_begin (v_prev
+ * from v_hist). Asynchronous on `stream`; the trace buffer is not written.
+ * Same result as the per-step calls, without a host round trip per step
+ * (reference counterpart: the reverse loop of vendor/ringfwi/elastic3d.py
+ * :386-463, which stores the whole history instead of recomputing). */
+int pe_solver_adjoint_segment(PeSolver *s, const PeState *state, const PeAdjoint *adj, void *v_hist,
+                              int64_t step_begin, int64_t step_end, const void *residual, void *stream);
+
 /* ---- Batches: many independent solves advanced together ----------------
  * No counterpart in the reference, which runs one azimuth at a time in a
  * Python loop (sim/pipeline/sweep_runner.py:322-390); the closest precedent

@@ -43,6 +43,8 @@ def _bind():
     if not getattr(L, "_adj_bound", False):
         L.pe_solver_adjoint_step.argtypes = [C.c_void_p, C.POINTER(_PeAdjoint), C.c_int64, C.c_void_p,
                                              C.c_void_p]
+        L.pe_solver_adjoint_segment.argtypes = [C.c_void_p, C.POINTER(_capi.PeState), C.POINTER(_PeAdjoint),
+                                                C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
         L._adj_bound = True
     return L
 
@@ -99,15 +101,10 @@ class AdjointSolve:
         for a in reversed(starts):
             b = min(a + self.K, nt)
             s.state.copy_(self.ckpt[a])
-            for n in range(a, b):
-                hist[n - a].copy_(s.state[:3])
-                s.run(n, n + 1)
-            for n in range(b - 1, a - 1, -1):
-                for i in range(3):
-                    adj.v_prev[i] = hist[n - a, i].data_ptr()
-                with torch.cuda.device(dev):
-                    _capi.check(L.pe_solver_adjoint_step(s._h, C.byref(adj), n, res.data_ptr(),
-                                                         C.c_void_p(stream.cuda_stream)))
+            # recompute the segment and step back through it in one C call
+            with torch.cuda.device(dev):
+                _capi.check(L.pe_solver_adjoint_segment(s._h, C.byref(s._st), C.byref(adj), hist.data_ptr(),
+                                                        a, b, res.data_ptr(), C.c_void_p(stream.cuda_stream)))
         s.check_status()
         return grad.cpu().numpy()
 

@@ -826,6 +826,50 @@ int pe_solver_adjoint_step(PeSolver *S, const PeAdjoint *adj, int64_t n, const v
                                   : adjoint_step_t<float>(S, adj, n, residual, st);
 }
 
+int pe_solver_adjoint_segment(PeSolver *S, const PeState *state, const PeAdjoint *adj0, void *v_hist,
+                              int64_t a, int64_t b, const void *residual, void *stream)
+{
+    if (!S || !state || !adj0 || !v_hist || !adj0->scratch || !adj0->grad)
+        return fail(PE_ERR_INVALID, "null adjoint argument");
+    for (int i = 0; i < 3; ++i)
+        if (!adj0->lv[i] || !state->v[i]) return fail(PE_ERR_INVALID, "adjoint velocity buffers missing");
+    for (int i = 0; i < 6; ++i)
+        if (!adj0->ls[i] || !state->s[i]) return fail(PE_ERR_INVALID, "adjoint stress buffers missing");
+    if (a < 0 || b <= a) return fail(PE_ERR_INVALID, "need 0 <= step_begin < step_end");
+    if (S->n_src > 0 && b > S->nt_wav) return fail(PE_ERR_INVALID, "step_end beyond the wavelet");
+    int rc = ensure_maps(S, state);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t fb = (size_t)S->esize * (size_t)S->ncell;   // bytes of one field
+    char *hist = (char *)v_hist;
+    // recompute the segment, keeping v before every step
+    for (int64_t n = a; n < b; ++n) {
+        for (int c = 0; c < 3; ++c)
+            PE_CUDA(cudaMemcpyAsync(hist + ((size_t)(n - a) * 3 + c) * fb, state->v[c], fb,
+                                    cudaMemcpyDeviceToDevice, st));
+        pe::k_step_set<<<1, 1, 0, st>>>(S->step, n);
+        if (S->cfg.dtype == PE_F64) {
+            pe::StepArgs<double> A = make_args<double>(S, state, 0);
+            launch_stress<double>(S, A, st);
+            launch_velocity<double>(S, A, st);
+        } else {
+            pe::StepArgs<float> A = make_args<float>(S, state, 0);
+            launch_stress<float>(S, A, st);
+            launch_velocity<float>(S, A, st);
+        }
+    }
+    PE_CUDA(cudaGetLastError());
+    // then the adjoint steps backwards through it
+    PeAdjoint adj = *adj0;
+    for (int64_t n = b - 1; n >= a; --n) {
+        for (int c = 0; c < 3; ++c) adj.v_prev[c] = hist + ((size_t)(n - a) * 3 + c) * fb;
+        rc = S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, &adj, n, residual, st)
+                                    : adjoint_step_t<float>(S, &adj, n, residual, st);
+        if (rc) return rc;
+    }
+    return PE_OK;
+}
+
 int pe_solver_status(PeSolver *S)
 {
     if (!S) return fail(PE_ERR_INVALID, "null solver");
