@@ -58,8 +58,11 @@ constexpr int PS_RING = 20;   // strain planes held
 constexpr size_t PS_SMEM_FIXED = 128 + sizeof(float) * ((size_t)PS_VSLOT + 2 * (size_t)PS_SSLOT + (size_t)PS_RING * PS_GST);
 constexpr int TAB36 = 36;   // material: columns J as [C0J..C3J] at 4J, then [C4J, C5J] at 24 + 2J
 // velocity
-constexpr int PV_OX = 32, PV_OY = 32;
-constexpr int PV_TW = 40, PV_TH = 40, PV_TSZ = PV_TW * PV_TH;     // s box with halo: 6400 B
+// two velocity blocks of 256 threads share an SM, so that one block's
+// barrier waits overlap the other's work
+constexpr int PV_ROWS = 16, PV_N = PR_LX * PV_ROWS;
+constexpr int PV_OX = 32, PV_OY = PV_ROWS;
+constexpr int PV_TW = 40, PV_TH = PV_OY + 8, PV_TSZ = PV_TW * PV_TH;   // s box with halo: 3840 B
 constexpr int PV_CSZ = PV_OX * PV_OY;                             // cell box: 4096 B
 constexpr int PV_SLOT = 5 * PV_TSZ + 4 * PV_CSZ;
 
@@ -768,7 +771,7 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
 }
 
 template <int NC>
-__global__ void __launch_bounds__(PR_N, 1) k_velocity_pair(const __grid_constant__ TmapsPairVelocity M,
+__global__ void __launch_bounds__(PV_N, 2) k_velocity_pair(const __grid_constant__ TmapsPairVelocity M,
                                                            const StepArgs<float> A, int n_mat)
 {
     extern __shared__ __align__(128) unsigned char smem_pair[];
@@ -781,7 +784,7 @@ __global__ void __launch_bounds__(PR_N, 1) k_velocity_pair(const __grid_constant
     }
     const bool rho_smem = pair_rho_in_smem(n_mat);
     if (rho_smem)
-        for (int i = tid; i < n_mat; i += PR_N) rsm[i] = A.rho[i];
+        for (int i = tid; i < n_mat; i += PV_N) rsm[i] = A.rho[i];
     __syncthreads();
     const float *rho_tab = rho_smem ? rsm : A.rho;
     const int zb = blockIdx.z * A.zc;
@@ -826,7 +829,7 @@ __global__ void __launch_bounds__(PR_N, 1)
 }
 
 template <int NC>
-__global__ void __launch_bounds__(PR_N, 1)
+__global__ void __launch_bounds__(PV_N, 2)
     k_velocity_pair_batch(const StepArgs<float> *__restrict__ descs, const TmapsPairVelocity *__restrict__ maps,
                           const int *__restrict__ n_mats, const BatchItem *__restrict__ items, int n_items,
                           int k)
@@ -848,7 +851,7 @@ __global__ void __launch_bounds__(PR_N, 1)
         const bool fresh = w.solve != cur;
         if (fresh) {
             copy_args(&As, descs + w.solve, k);
-            for (int i = threadIdx.x; i < n_mats[w.solve]; i += PR_N) rsm[i] = As.rho[i];
+            for (int i = threadIdx.x; i < n_mats[w.solve]; i += PV_N) rsm[i] = As.rho[i];
         }
         __syncthreads();
         const int zb = w.bz * As.zc;

@@ -231,9 +231,9 @@ void launch_velocity(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t 
             dim3 grid((A.nx + pe::PV_OX - 1) / pe::PV_OX, (A.ny + pe::PV_OY - 1) / pe::PV_OY, (A.nz + A.zc - 1) / A.zc);
             const size_t sm = pe::velocity_pair_smem(S->cfg.n_mat);
             if (A.nc == 4)
-                pe::k_velocity_pair<4><<<grid, pe::PR_N, sm, st>>>(S->mpv, A, S->cfg.n_mat);
+                pe::k_velocity_pair<4><<<grid, pe::PV_N, sm, st>>>(S->mpv, A, S->cfg.n_mat);
             else
-                pe::k_velocity_pair<0><<<grid, pe::PR_N, sm, st>>>(S->mpv, A, S->cfg.n_mat);
+                pe::k_velocity_pair<0><<<grid, pe::PV_N, sm, st>>>(S->mpv, A, S->cfg.n_mat);
             return;
         }
     }
@@ -410,7 +410,7 @@ int configure_kernels(PeSolver *S)
             const long long tps = (long long)((c.nx + pe::PS_OX) / pe::PS_OX) * ((c.ny + pe::PS_OY - 1) / pe::PS_OY);
             const long long tpv = (long long)((c.nx + pe::PV_OX - 1) / pe::PV_OX) * ((c.ny + pe::PV_OY - 1) / pe::PV_OY);
             const int sps = occupancy_slots(pe::k_stress_pair<4, true>, pe::PR_N, ps);
-            const int spv = occupancy_slots(pe::k_velocity_pair<4>, pe::PR_N, pv);
+            const int spv = occupancy_slots(pe::k_velocity_pair<4>, pe::PV_N, pv);
             S->zc_ps = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tps, sps, 3);
             S->zc_pv = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tpv, spv, 2);
         }
@@ -1115,8 +1115,10 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
                 for (int bx = 0; bx < (c.nx + pe::PV_OX - 1) / pe::PV_OX; ++bx) iv.push_back({s, bx, by, bz});
         }
     }
+    int per_v = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_v, pe::k_velocity_pair_batch<4>, pe::PV_N, B->smem_v);
     B->grid_s = std::max(1, std::min((int)is.size(), nsm));
-    B->grid_v = std::max(1, std::min((int)iv.size(), nsm));
+    B->grid_v = std::max(1, std::min((int)iv.size(), nsm * std::max(1, per_v)));
     return PE_OK;
 }
 
@@ -1266,9 +1268,9 @@ int batch_chunk(PeBatch *B, int len)
                 else
                     pe::k_stress_pair_batch<0, false><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
                 if (B->pair_nc4)
-                    pe::k_velocity_pair_batch<4><<<B->grid_v, pe::PR_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
+                    pe::k_velocity_pair_batch<4><<<B->grid_v, pe::PV_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
                 else
-                    pe::k_velocity_pair_batch<0><<<B->grid_v, pe::PR_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
+                    pe::k_velocity_pair_batch<0><<<B->grid_v, pe::PV_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
                 B->launches += 2;
             }
         }
