@@ -11,9 +11,9 @@
 //  - the half-cell moves read strain rows as 64-bit pairs (42 loads per pair
 //    of cells instead of 156 scalar loads);
 //  - the stiffness product runs column by column (J outer), reading column J
-//    of a material from a shared-memory (n_mat, 36) table with one 128-bit
-//    and one 64-bit load per cell, which keeps the register footprint within
-//    the 512-thread budget;
+//    of a material from a (n_mat, 36) table (shared memory when two blocks'
+//    copies fit, else through L1) with one 128-bit and one 64-bit load per
+//    cell, which keeps the register footprint within 128 registers;
 //  - tiles whose every tap lies inside the grid run an unguarded body; the
 //    others zero the coefficients of skipped taps instead of branching.
 // Data movement is the TMA scheme of the one-column kernels: one elected
@@ -21,25 +21,28 @@
 // mbarrier-tracked slots; z taps come from per-thread register rings.
 // Every mbarrier wait is bounded (status word, no hang).
 //
-// Block: 512 threads = 16 lanes along x (two columns each) x 32 rows.
-//   k_stress_pair    strain tile 32 x 32 columns, the inner 30 x 30 are
+// Blocks: 256 threads = 16 lanes along x (two columns each) x 16 rows, two
+// blocks per SM, so that one block's barrier and memory waits overlap the
+// other's work.
+//   k_stress_pair    strain tile 32 x 16 columns, the inner 30 x 14 are
 //                    updated; replaces strains_zp + stress_lab_u + the source
 //                    scatter (sim/core/fdtd.py:1102-1177, :594-689,
 //                    :1798-1800).
-//   k_velocity_pair  32 x 32 cells; replaces vel_zp and the receiver gather
+//   k_velocity_pair  32 x 16 cells; replaces vel_zp and the receiver gather
 //                    (sim/core/fdtd.py:1179-1257, :1806-1813).
 #pragma once
 #include "pe_kernels_tma.cuh"
 
 namespace pe {
 
-constexpr int PR_LX = 16, PR_ROWS = 32, PR_N = PR_LX * PR_ROWS;   // 512 threads
-// stress
-constexpr int PS_OX = 30, PS_OY = 30;                             // updated cells per block
-constexpr int PS_VW = 44, PS_VH = 40, PS_VSZ = PS_VW * PS_VH;     // v box: 1760 floats (7040 B)
-constexpr int PS_SW = 36, PS_SH = 30, PS_SSZ = PS_SW * PS_SH;     // cell box: 1080 floats
-constexpr int PS_SSZP = 1088;                                     // ... padded to 128 B
-constexpr int PS_GW = 32, PS_GOFF = 8, PS_GST = 1040;             // strain plane: pad, 32 x 32, pad
+constexpr int PR_LX = 16;                                         // lanes along x, two columns each
+// stress: two 256-thread blocks per SM (16 rows of strain columns)
+constexpr int PS_ROWS = 16, PS_N = PR_LX * PS_ROWS;
+constexpr int PS_OX = 30, PS_OY = PS_ROWS - 2;                    // updated cells per block
+constexpr int PS_VW = 44, PS_VH = PS_ROWS + 8, PS_VSZ = PS_VW * PS_VH;   // v box: 1056 floats (4224 B)
+constexpr int PS_SW = 36, PS_SH = PS_OY, PS_SSZ = PS_SW * PS_SH;  // cell box: 504 floats
+constexpr int PS_SSZP = 512;                                      // ... padded to 128 B
+constexpr int PS_GW = 32, PS_GOFF = 8, PS_GST = 2 * PS_GOFF + PS_GW * PS_ROWS;   // strain plane: pad, 32 x 16, pad
 constexpr int PS_VSLOT = 3 * PS_VSZ;
 constexpr int PS_SSLOT = 6 * PS_SSZP;
 // Strain ring: the update of plane z reads g4 and g5 at planes z - 1 and z,
@@ -77,10 +80,12 @@ struct alignas(64) TmapsPairVelocity {
     CUtensorMap dv;      // damping volume: box 32 x 32
 };
 
-// the table goes to shared memory when it fits the 227 KB opt-in limit
+// the table goes to shared memory when two blocks with it still fit an
+// SM's 228 KB (1 KB of each block's share is reserved), else it is read
+// through L1
 __host__ __device__ constexpr bool pair_tab_in_smem(int n_mat)
 {
-    return PS_SMEM_FIXED + (size_t)n_mat * TAB36 * sizeof(float) <= 232448;
+    return 2 * (PS_SMEM_FIXED + (size_t)n_mat * TAB36 * sizeof(float) + 1024) <= 233472;
 }
 __host__ __device__ constexpr size_t stress_pair_smem(int n_mat)
 {
@@ -361,7 +366,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     tl.yf = lim_f(gy, ny);
     mg.ylo = gy >= 1;
     mg.yhi = gy <= ny - 2;
-    // updated cells: inner 30 x 30 of the strain tile, inside the grid
+    // updated cells: inner 30 x 14 of the strain tile, inside the grid
     const bool row_out = r >= 1 && r <= PS_OY && gy < ny;
     bool out_c[2];
     out_c[0] = row_out && l >= 1 && gx0 >= 0 && gx0 < nx;
@@ -374,7 +379,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         dxx[1] = A.dx[gx0 + 1];
     }
     const bool tile_in = S0 - T_H >= 0 && S0 + PS_GW - 1 + T_H < nx && S0y - T_H >= 0 &&
-                         S0y + PR_ROWS - 1 + T_H < ny;
+                         S0y + PS_ROWS - 1 + T_H < ny;
     // a warp's two rows both past the last grid row: no strain of theirs is
     // read by an updated cell, so the warp skips the strain work (warp-uniform)
     const bool warp_rows_in = S0y + 2 * (tid >> 5) < ny;
@@ -539,7 +544,7 @@ __device__ __forceinline__ void stress_pair_init(unsigned char *smem)
 // at the same time march the same planes of neighbouring tiles, so the tile
 // halos they share are read from DRAM once and from L2 after that.
 template <int NC, bool TS>
-__global__ void __launch_bounds__(PR_N, 1) k_stress_pair(const __grid_constant__ TmapsPairStress M,
+__global__ void __launch_bounds__(PS_N, 2) k_stress_pair(const __grid_constant__ TmapsPairStress M,
                                                          const StepArgs<float> A,
                                                          const float *__restrict__ tab36, int n_mat)
 {
@@ -799,7 +804,7 @@ __global__ void __launch_bounds__(PV_N, 2) k_velocity_pair(const __grid_constant
 // re-staging the solve's arguments and tables only when the solve changes.
 // All solves of a pair batch have rows of 16-byte multiples.
 template <int NC, bool TS>
-__global__ void __launch_bounds__(PR_N, 1)
+__global__ void __launch_bounds__(PS_N, 2)
     k_stress_pair_batch(const StepArgs<float> *__restrict__ descs, const TmapsPairStress *__restrict__ maps,
                         const float *const *__restrict__ tabs, const int *__restrict__ n_mats,
                         const BatchItem *__restrict__ items, int n_items, int k)

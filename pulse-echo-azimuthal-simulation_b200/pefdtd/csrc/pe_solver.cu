@@ -197,10 +197,10 @@ void launch_stress(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st
             const int nm = S->cfg.n_mat;
             const size_t sm = pe::stress_pair_smem(nm);
             const bool ts = pe::pair_tab_in_smem(nm);
-            if (A.nc == 4 && ts) pe::k_stress_pair<4, true><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
-            else if (A.nc == 4) pe::k_stress_pair<4, false><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
-            else if (ts) pe::k_stress_pair<0, true><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
-            else pe::k_stress_pair<0, false><<<grid, pe::PR_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            if (A.nc == 4 && ts) pe::k_stress_pair<4, true><<<grid, pe::PS_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            else if (A.nc == 4) pe::k_stress_pair<4, false><<<grid, pe::PS_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            else if (ts) pe::k_stress_pair<0, true><<<grid, pe::PS_N, sm, st>>>(S->mps, A, S->tab36, nm);
+            else pe::k_stress_pair<0, false><<<grid, pe::PS_N, sm, st>>>(S->mps, A, S->tab36, nm);
             return;
         }
     }
@@ -409,7 +409,7 @@ int configure_kernels(PeSolver *S)
             PE_CUDA(cudaFuncSetAttribute(pe::k_velocity_pair<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             const long long tps = (long long)((c.nx + pe::PS_OX) / pe::PS_OX) * ((c.ny + pe::PS_OY - 1) / pe::PS_OY);
             const long long tpv = (long long)((c.nx + pe::PV_OX - 1) / pe::PV_OX) * ((c.ny + pe::PV_OY - 1) / pe::PV_OY);
-            const int sps = occupancy_slots(pe::k_stress_pair<4, true>, pe::PR_N, ps);
+            const int sps = occupancy_slots(pe::k_stress_pair<4, true>, pe::PS_N, ps);
             const int spv = occupancy_slots(pe::k_velocity_pair<4>, pe::PV_N, pv);
             S->zc_ps = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tps, sps, 3);
             S->zc_pv = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tpv, spv, 2);
@@ -1084,7 +1084,8 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
     cudaFuncAttributes fa{};
     PE_CUDA(cudaFuncGetAttributes(&fa, pe::k_stress_pair_batch<4, true>));
     const size_t dyn_s = (size_t)optin - fa.sharedSizeBytes;
-    B->pair_ts = pe::PS_SMEM_FIXED + (size_t)max_mat * pe::TAB36 * sizeof(float) <= dyn_s;
+    B->pair_ts = pe::pair_tab_in_smem(max_mat) &&
+                 pe::PS_SMEM_FIXED + (size_t)max_mat * pe::TAB36 * sizeof(float) <= dyn_s;
     B->smem_s = pe::PS_SMEM_FIXED + (B->pair_ts ? (size_t)max_mat * pe::TAB36 * sizeof(float) : 0);
     B->smem_v = 128 + sizeof(float) * (3 * (size_t)pe::PV_SLOT + (size_t)max_mat);
     PE_CUDA(cudaFuncGetAttributes(&fa, pe::k_velocity_pair_batch<4>));
@@ -1115,9 +1116,10 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
                 for (int bx = 0; bx < (c.nx + pe::PV_OX - 1) / pe::PV_OX; ++bx) iv.push_back({s, bx, by, bz});
         }
     }
-    int per_v = 1;
+    int per_v = 1, per_s = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_v, pe::k_velocity_pair_batch<4>, pe::PV_N, B->smem_v);
-    B->grid_s = std::max(1, std::min((int)is.size(), nsm));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, pe::k_stress_pair_batch<4, true>, pe::PS_N, B->smem_s);
+    B->grid_s = std::max(1, std::min((int)is.size(), nsm * std::max(1, per_s)));
     B->grid_v = std::max(1, std::min((int)iv.size(), nsm * std::max(1, per_v)));
     return PE_OK;
 }
@@ -1260,13 +1262,13 @@ int batch_chunk(PeBatch *B, int len)
                 const pe::StepArgs<float> *d = (const pe::StepArgs<float> *)B->descs;
                 const int ns = B->n_items_s, nv = B->n_items_v;
                 if (B->pair_nc4 && B->pair_ts)
-                    pe::k_stress_pair_batch<4, true><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                    pe::k_stress_pair_batch<4, true><<<B->grid_s, pe::PS_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
                 else if (B->pair_nc4)
-                    pe::k_stress_pair_batch<4, false><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                    pe::k_stress_pair_batch<4, false><<<B->grid_s, pe::PS_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
                 else if (B->pair_ts)
-                    pe::k_stress_pair_batch<0, true><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                    pe::k_stress_pair_batch<0, true><<<B->grid_s, pe::PS_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
                 else
-                    pe::k_stress_pair_batch<0, false><<<B->grid_s, pe::PR_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
+                    pe::k_stress_pair_batch<0, false><<<B->grid_s, pe::PS_N, B->smem_s, B->stream>>>(d, B->pmaps_s, B->tabs, B->nmats, B->items_s, ns, k);
                 if (B->pair_nc4)
                     pe::k_velocity_pair_batch<4><<<B->grid_v, pe::PV_N, B->smem_v, B->stream>>>(d, B->pmaps_v, B->nmats, B->items_v, nv, k);
                 else
