@@ -186,7 +186,7 @@ typedef struct PeAdjoint {
     void *lv[3];             /* adjoint of vx, vy, vz */
     void *ls[6];             /* adjoint of s1..s6 */
     const void *v_prev[3];   /* forward v^{n-1} */
-    void *scratch;           /* 15 fields of (nz, ny, nx) */
+    void *scratch;           /* 33 fields of (nz, ny, nx) */
     double *grad;            /* (n_mat, 21) dJ/dC upper triangle, accumulated */
 } PeAdjoint;
 

@@ -86,7 +86,7 @@ class AdjointSolve:
         L = _bind()
         with torch.cuda.device(dev):
             lam = torch.zeros((9,) + shape, dtype=tdt, device=dev)
-            scratch = torch.zeros((15,) + shape, dtype=tdt, device=dev)
+            scratch = torch.zeros((33,) + shape, dtype=tdt, device=dev)
             grad = torch.zeros((s.cfg.n_mat, 21), dtype=torch.float64, device=dev)
             hist = torch.empty((min(self.K, nt), 3) + shape, dtype=tdt, device=dev)
         adj = _PeAdjoint()

@@ -11,6 +11,8 @@
 //   k_adj_vel_u     u = d dt_h lv / rho_face              (per component)
 //   k_adj_vel       ls += G^T u                           (gathers)
 //   k_adj_strain    g = D v^{n-1}                         (same taps as forward)
+//   k_adj_w         w[p][J] = sum over stresses I at position p of
+//                   C_IJ dt ls_I, for the 18 moved (p, J), once per cell
 //   k_adj_stress    dJ/dC[m] += dt ls (x) (M g); t = M^T C^T (dt ls)
 //   k_adj_velfin    lv = d lv + D^T t
 //   k_adj_damp      ls = d ls
@@ -33,6 +35,7 @@ struct AdjArgs {
     T *u[3];           // scratch: scaled velocity adjoint
     T *g[6];           // scratch: forward strains
     T *t[6];           // scratch: strain adjoint
+    T *w[18];          // scratch: C^T (dt ls) per moved (position, strain)
     const uint16_t *lab;
     const T *c21;      // (n_mat, C21_STRIDE)
     const T *rho;
@@ -207,6 +210,39 @@ __device__ __forceinline__ bool move_ok(int z, int y, int x, int dz, int dy, int
 }
 
 // ---------------------------------------------------------------- stress transpose
+// index of the moved (position p, strain J) pairs, p != position of J:
+// J = 0..5 in order, p ascending, three per strain
+__host__ __device__ constexpr int adj_widx(int J, int p)
+{
+    return 3 * J + (p - (p > (J < 3 ? 0 : J - 2) ? 1 : 0));
+}
+
+// w[p][J](x) = sum over I at position p of C_IJ(x) * (dt * ls_I(x)), I
+// ascending, for the moved pairs: the values the stress transpose gathers
+// from the forward cells of each move tap
+template <typename T>
+__global__ void k_adj_w(AdjArgs<T> A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    const int VP[6] = {0, 0, 0, 1, 2, 3};
+    const T *Cx = A.c21 + (long long)(A.lab[i] & LAB_MAT) * C21_STRIDE;
+    T e[6];
+#pragma unroll
+    for (int I = 0; I < 6; ++I) e[I] = A.dt * A.ls[I][i];
+#pragma unroll
+    for (int J = 0; J < 6; ++J)
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p == VP[J]) continue;
+            T W = 0;
+#pragma unroll
+            for (int I = 0; I < 6; ++I)
+                if (VP[I] == p) W += Cx[c21_slot(I, J)] * e[I];
+            A.w[adj_widx(J, p)][i] = W;
+        }
+}
+
 template <typename T>
 __global__ void k_adj_stress(AdjArgs<T> A)
 {
@@ -279,11 +315,7 @@ __global__ void k_adj_stress(AdjArgs<T> A)
                             const int xz = iz - a0, xy = iy - a1, xx = ix - a2;
                             if (!move_ok(xz, xy, xx, dz, dy, dx, nz, ny, nx)) continue;
                             const long long xi = i - a0 * sz - a1 * sy - a2;
-                            const T *Cx = A.c21 + (long long)(A.lab[xi] & LAB_MAT) * C21_STRIDE;
-                            T W = 0;
-                            for (int I = 0; I < 6; ++I)
-                                if (VP[I] == p) W += Cx[c21_slot(I, J)] * (A.dt * A.ls[I][xi]);
-                            acc += T(0.25) * W;
+                            acc += T(0.25) * A.w[adj_widx(J, p)][xi];
                         }
             }
             tJ[J] = acc;

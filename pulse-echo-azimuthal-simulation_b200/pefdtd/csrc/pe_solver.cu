@@ -774,6 +774,7 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
         A.g[i] = (T *)adj->scratch + (size_t)(3 + i) * ncell;
         A.t[i] = (T *)adj->scratch + (size_t)(9 + i) * ncell;
     }
+    for (int k = 0; k < 18; ++k) A.w[k] = (T *)adj->scratch + (size_t)(15 + k) * ncell;
     A.lab = S->lab;
     A.c21 = (const T *)S->c21;
     A.rho = (const T *)S->rho;
@@ -802,6 +803,7 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
     pe::k_adj_vel_u<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_vel<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_strain<T><<<nb, 256, 0, st>>>(A);
+    pe::k_adj_w<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_stress<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_velfin<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_damp<T><<<nb, 256, 0, st>>>(A);
