@@ -178,9 +178,10 @@ def _e2e(p, steps):
             "steps": steps, "wall_s": el, "api": "pe_forward_host (C ABI, host buffers)"}
 
 
-def _cpu_run(p, budget_s, max_steps):
+def _cpu_run(p, budget_s, max_steps, warmup=3):
     """Reference kernels on the host (oracle/_ref), else the C oracle port;
-    time-boxed. Returns (Gcell/s, steps, cores, kind, sample)."""
+    `warmup` untimed steps (which also size the sample), then a time-boxed
+    timed run. Returns (Gcell/s, steps, cores, kind, sample)."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     ncell = int(np.prod(p["lab"].shape))
@@ -199,7 +200,8 @@ def _cpu_run(p, budget_s, max_steps):
             O.run_oracle(pr, n_threads=cores)
         return time.perf_counter() - t0
 
-    t1 = run(1)                         # warm-up + sizing
+    w = max(1, int(warmup))
+    t1 = run(w) / w                     # warm-up steps, which also size the sample
     n = int(max(2, min(max_steps, len(p["wavelet"]), budget_s / max(t1, 1e-3))))
     el = run(n)
     which = ("the reference's dense update kernels (strains, stress_acc, vel_update)"
@@ -299,10 +301,11 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        p = _problem(args.workload, nt=max(K, 8))
-        val, n, cores, kind, sample = _cpu_run(p, budget_s=90.0, max_steps=K)
+        p = _problem(args.workload, nt=max(K, W, 8))
+        val, n, cores, kind, sample = _cpu_run(p, budget_s=90.0, max_steps=K, warmup=W)
         line = {"metric": "Gcell-updates/s", "value": val, "unit": "Gcell-updates/s",
-                "n_gpus": args.gpus, "steps": n, "warmup": 1, "ms_per_step": None,
+                "n_gpus": args.gpus, "steps": n, "warmup": W,
+                "ms_per_step": int(np.prod(p["lab"].shape)) / (val * 1e9) * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "impl": "reference",
                 "config": {"workload": args.workload, "grid": list(p["lab"].shape),
