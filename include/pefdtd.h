@@ -256,6 +256,47 @@ int pe_label_cylinder(const double *xs, int nx, const double *ys, int ny, const 
 int pe_rotated_grid(const int32_t *labels_dev, int nx_s, int nz_s, double h_spec, double h, int nd,
                     int ndz, double cos_a, double sin_a, int m, int32_t *out_dev, void *stream);
 
+/* Batched trace post-processing, float64 on the device. A batch is `batch`
+ * traces packed back to back in one device array: trace i is samples
+ * off[i] .. off[i+1]-1 (off: host int64 (batch + 1), off[0] = 0, every trace
+ * non-empty). x_dev is PE_F32 or PE_F64 (`dtype`); results are device f64.
+ * Window bounds, time steps and filter coefficients come from the host,
+ * computed as the reference's Python computes them. All synchronous on
+ * `stream`.
+ *
+ * pe_trace_envelope: env = |x + i H(x)| with H the discrete Hilbert
+ * transform of the whole trace (scipy.signal.hilbert, as used by
+ * sim/core/fdtd.py:976 and sim/pipeline/sweep_runner.py:210). */
+int pe_trace_envelope(const void *x_dev, int32_t dtype, const int64_t *off, int32_t batch, double *env_dev,
+                      void *stream);
+
+/* pe_trace_detrend: n_ab == 0: x - mean(x) per trace (sim/core/fdtd.py:974);
+ * else filtfilt(b, a, x) with odd padding of `padlen` samples at each end and
+ * initial state zi * (first sample) (scipy.signal.filtfilt defaults; the
+ * reference's detrend_hp, sim/core/fdtd.py:943-948). b, a: host (n_ab,)
+ * normalised so a[0] = 1, 2 <= n_ab <= 8; zi: host (n_ab - 1,)
+ * (scipy.signal.lfilter_zi); padlen <= 24 and every trace longer than padlen. */
+int pe_trace_detrend(const void *x_dev, int32_t dtype, const int64_t *off, int32_t batch, const double *b,
+                     const double *a, int32_t n_ab, const double *zi, int32_t padlen, double *out_dev,
+                     void *stream);
+
+/* pe_trace_pick: envelope peak in [lo, hi) per trace (win: host int64
+ * (batch, 2), hi > lo + 2), first index on ties, parabolic refinement;
+ * out_dev (batch, 3): pick time (refined index * dt[i]), peak value, and 1.0
+ * when the peak is not on a window edge (sim/core/fdtd.py:977-984). */
+int pe_trace_pick(const double *env_dev, const int64_t *off, int32_t batch, const int64_t *win, const double *dt,
+                  double *out_dev, void *stream);
+
+/* pe_trace_analyse: the sweep driver's per-trace figures
+ * (sim/pipeline/sweep_runner.py:209-225). win: host int64 (batch, 4) = E1
+ * window [a, b) (b > a) and coda window [lo, hi); dt_fs: host (batch, 2) =
+ * dt and 1/dt. out_dev (batch, 4): E1 (envelope max in [a, b)), t1 (its
+ * index * dt), coda = 20 log10(sqrt(mean(env[lo:hi]^2)) / E1 + 1e-30) and
+ * tail = max |x[k:]| / max(E1, 1e-30) with k = int((t1 + 3e-6) * fs), NaN
+ * unless k < n - 8. */
+int pe_trace_analyse(const void *x_dev, int32_t dtype, const double *env_dev, const int64_t *off, int32_t batch,
+                     const int64_t *win, const double *dt_fs, double *out_dev, void *stream);
+
 /* Allocation-free variant of pe_label_cylinder, with no counterpart in the
  * reference. For callers that may not allocate device memory (an application
  * whose framework has reserved the device pool for its own allocator, or a

@@ -96,6 +96,15 @@ def lib():
                                         C.c_void_p, C.c_void_p]
         L.pe_rotated_grid.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                       C.c_int, C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+        L.pe_trace_envelope.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                        C.c_void_p]
+        L.pe_trace_detrend.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                       C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                       C.c_void_p]
+        L.pe_trace_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
+        L.pe_trace_analyse.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         if L.pe_abi_version() != ABI_VERSION:
             raise RuntimeError("pefdtd library ABI mismatch; rebuild with pefdtd.build")
         _lib = L
@@ -116,6 +125,8 @@ def ptr(a):
     """Host address of a contiguous numpy array (or None)."""
     if a is None:
         return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array handed to the C ABI must be C-contiguous")
     return a.ctypes.data_as(C.c_void_p).value
 
 
@@ -125,4 +136,5 @@ def exported_symbols():
             "pe_solver_destroy",
             "pe_forward_host", "pe_label_cylinder", "pe_rotated_grid", "pe_batch_create", "pe_batch_schedule",
             "pe_batch_set_wavelet", "pe_batch_run", "pe_batch_status", "pe_batch_launch_count",
-            "pe_batch_destroy"]
+            "pe_batch_destroy", "pe_trace_envelope", "pe_trace_detrend", "pe_trace_pick",
+            "pe_trace_analyse"]

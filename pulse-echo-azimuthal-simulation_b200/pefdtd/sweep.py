@@ -193,10 +193,12 @@ def analyse(tr, dt):
     return wavelets.analyse_trace(tr, dt, path_m=0.200, c_ref=C_REF)
 
 
-def save_azimuth(cfg, az, tr, dt, f0, h, root=None):
+def save_azimuth(cfg, az, tr, dt, f0, h, root=None, analysis=None):
+    """Write az{ddd}.npz; ``analysis`` = (E1, t1, coda, tail) computed
+    elsewhere (the device batch analysis), else computed here on the host."""
     d = sweep_dir(cfg["name"], _root_of(cfg, root))
     tr = np.asarray(tr, float).ravel()
-    E1, t1, coda, tail = analyse(tr, dt)
+    E1, t1, coda, tail = analyse(tr, dt) if analysis is None else analysis
     tmp = os.path.join(d, f"az{az:03d}.tmp.npz")
     np.savez(tmp, trace=tr.astype(np.float32), dt=dt, f0=f0, az_deg=az, E1=E1, t1_s=t1,
              coda_db=coda, tail=tail, h=h, order=cfg["order"], ppw=cfg["ppw"],
@@ -316,7 +318,11 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
     as many as fit in device memory). ``labeller``: see
     specimen.DiskSpecimen.build. ``solver``: callable(setups, progress) ->
     traces; the GPU batch solver unless replaced (tests drive the file
-    protocol on CPU with a stand-in). ``rank``/``world``: one process per
+    protocol on CPU with a stand-in). With the GPU solver each batch's
+    figures (E1, t1, coda, tail) are computed on the device
+    (:func:`pefdtd.traces.analyse`: t1 identical to the host analysis, the
+    others to ~1e-13 relative); with a stand-in, on the host, exactly as the
+    reference computes them. ``rank``/``world``: one process per
     GPU; each rank solves its share of the pending azimuths
     (:func:`pefdtd.shard.assign`, every azimuth of a sweep costs the same)
     and writes their files; rank 0 alone writes status.json."""
@@ -325,6 +331,7 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
         status = lambda *a, **k: None  # noqa: E731,F841  (rank 0 owns status.json)
     else:
         status = globals()["status"]
+    device_analysis = solver is None
     if solver is None:
         try:
             import torch
@@ -436,8 +443,16 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
                 status(cfg, root, phase="stopped")
                 result = "stopped"
                 break
-            for s, tr in zip(cur, traces):
-                E1, t1, coda, tail = save_azimuth(cfg, s["az"], tr, s["dt"], s["f0"], s["h"], root)
+            if device_analysis:
+                # the batch's E1 / arrival / coda / tail in one device pass
+                from . import traces as trace_ops
+                figs = trace_ops.analyse(traces, [s["dt"] for s in cur], path_m=0.200, c_ref=C_REF,
+                                         device=device)
+            else:
+                figs = [None] * len(cur)
+            for s, tr, fig in zip(cur, traces, figs):
+                E1, t1, coda, tail = save_azimuth(cfg, s["az"], tr, s["dt"], s["f0"], s["h"], root,
+                                                  analysis=fig)
                 log(f"[sweep] az {s['az']:3d}: coda {coda:6.1f} dB, E1 {E1:.4g}, "
                     f"ToF {t1 * 1e6:.3f} us, tail {tail:.3f} "
                     f"({'STABLE' if tail < 0.5 else 'CHECK'})")

@@ -46,6 +46,11 @@ def test_batched_sweep_matches_single_solves_and_oracle(tmp_path):
         with np.load(os.path.join(tmp_path, "g", f"az{az:03d}.npz")) as z:
             assert np.array_equal(z["trace"], single[:, 0].astype(np.float32))
             assert float(z["dt"]) == s["dt"] and len(z["trace"]) == s["nt"]
+            # figures from the device analysis against the host (reference) one
+            E1, t1, coda, tail = sweep.analyse(np.asarray(z["trace"], float), s["dt"])
+            assert float(z["t1_s"]) == t1 and abs(float(z["E1"]) - E1) <= 1e-11 * E1
+            assert abs(float(z["coda_db"]) - coda) <= 1e-9
+            assert (np.isnan(tail) and np.isnan(float(z["tail"]))) or abs(float(z["tail"]) - tail) <= 1e-11 * tail
         if k == 0:
             from oracle.oracle import problem_from_workload
             p = dict(lab=lab, mats=spec["mats"], Ct=spec["Ct"], rho_t=spec["rho_t"], h=s["h"],
