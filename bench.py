@@ -281,6 +281,95 @@ def _sweep(args):
                        "timing": "wall clock, set-up and trace download included, synchronised"}}
 
 
+def _traces(args):
+    """Device vs host post-processing of N records of the workload's length
+    (sweep analysis and high-passed picks; one line of JSON)."""
+    import torch
+    from pefdtd import traces, wavelets
+    n, N, dt = 6000, int(args.traces), 1.0e-8
+    rng = np.random.default_rng(7)
+    t = np.arange(n) * dt
+    host = []
+    for i in range(N):
+        x = 0.2 + 0.01 * rng.standard_normal(n)
+        tau = t - (51.9e-6 + 0.3e-6 * rng.standard_normal())
+        m = (tau >= 0) & (tau <= 2.2e-6)
+        x[m] += 0.5 * (1 - np.cos(2 * np.pi * tau[m] / 2.2e-6)) * np.sin(2 * np.pi * 2.25e6 * tau[m])
+        host.append(x.astype(np.float32))
+    dev = [torch.from_numpy(x).cuda() for x in host]
+
+    def device_pass():
+        a = traces.analyse(dev, dt)
+        p = traces.pick_peaks(t, dev, t_lo=30e-6, f_lo=0.3e6)
+        return a, p
+
+    for _ in range(3):
+        device_pass()
+    torch.cuda.synchronize()
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        a_dev, p_dev = device_pass()
+    torch.cuda.synchronize()
+    t_dev = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    a_host = [wavelets.analyse_trace(np.asarray(x, float), dt) for x in host]
+    p_host = [wavelets.pick_peak(t, x, t_lo=30e-6, dt=dt, f_lo=0.3e6) for x in host]
+    t_host = time.perf_counter() - t0
+    same_t1 = all(a[1] == b[1] for a, b in zip(a_dev, a_host))
+    same_pick = all(abs(a[0] - b[0]) <= 1e-6 * dt and a[2] == b[2] for a, b in zip(p_dev, p_host))
+    return {"metric": "traces post-processed/s (analysis + high-passed pick)", "unit": "traces/s",
+            "traces": N, "samples": n, "device": N / t_dev, "host": N / t_host,
+            "speedup": t_host / t_dev, "device_ms": t_dev * 1e3, "host_ms": t_host * 1e3,
+            "host_cores": 1, "arrivals_identical": bool(same_t1), "picks_identical": bool(same_pick),
+            "config": {"timing": "wall clock; device: f32 records resident on the GPU, results read back; "
+                                 "host: the reference's SciPy computations, one thread"}}
+
+
+def _gradients(args):
+    """Misfits and stiffness gradients of N solves: one at a time vs
+    pefdtd.adjoint.misfit_gradients (one line of JSON)."""
+    import torch
+    from pefdtd import workloads
+    from pefdtd.adjoint import Problem, misfit_gradients
+    from pefdtd.fdtd import _material_tables64
+    from pefdtd.materials import c36_to_c21
+    K = int(args.steps)
+    probs, c21s, dobs, cells = [], [], [], 0
+    for i in range(int(args.gradients)):
+        spec = dict(workloads.WORKLOADS[args.workload], seed=11 + i)
+        p = workloads.make_problem(spec, nt=K)
+        probs.append(Problem(p["mats"], p["rho_t"], p["h"], p["dt"], p["coeffs"], p["src_pts"],
+                             p["rec_groups"], p["wavelet"], record="vz", sponge_width=p["sponge"],
+                             dtype="float32", checkpoint_every=200))
+        c21s.append(c36_to_c21(_material_tables64(p["axes"], 1500.0, 300.0)[0]))
+        dobs.append(np.zeros((K, 1)))
+        cells += int(np.prod(p["lab"].shape))
+    misfit_gradients(probs[:1], c21s[:1], dobs[:1])   # warm-up (library, allocator)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = []
+    for pr, c, d in zip(probs, c21s, dobs):
+        a = pr.make_adjoint(c)
+        tr = a.forward().to(torch.float64)
+        r = tr - torch.as_tensor(d, device=tr.device)
+        plain.append(a.backward(r))
+        a.solve.close()
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    got = misfit_gradients(probs, c21s, dobs)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    dev = max(float(np.abs(g - q).max() / max(np.abs(q).max(), 1e-300)) for (_, g), q in zip(got, plain))
+    return {"metric": "misfit + gradient solves/s, batched vs plain loop", "unit": "solves/s",
+            "solves": len(probs), "steps": K, "cells_per_solve": cells // len(probs),
+            "plain": len(probs) / t_plain, "batched": len(probs) / t_batch, "speedup": t_plain / t_batch,
+            "plain_s": t_plain, "batched_s": t_batch, "max_rel_grad_diff": dev,
+            "config": {"workload": args.workload, "dtype": "f32", "checkpoint_every": 200,
+                       "timing": "wall clock; solver creation, forward, adjoint and gradient download included"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -292,6 +381,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--sweep", type=int, default=0)
     ap.add_argument("--uneven", action="store_true")
+    ap.add_argument("--traces", type=int, default=0)
+    ap.add_argument("--gradients", type=int, default=0)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -320,6 +411,14 @@ def main():
     if args.sweep:
         if rank == 0:
             print(json.dumps(_sweep(args)), flush=True)
+        return
+    if args.traces:
+        if rank == 0:
+            print(json.dumps(_traces(args)), flush=True)
+        return
+    if args.gradients:
+        if rank == 0:
+            print(json.dumps(_gradients(args)), flush=True)
         return
 
     import torch

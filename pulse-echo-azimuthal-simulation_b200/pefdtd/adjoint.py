@@ -16,6 +16,8 @@ vendor/ringfwi/axisfield.py:37-161. Here:
   backward is that adjoint with the incoming trace gradient as the adjoint
   source, so any loss on the traces (``0.5*||tr - d||^2`` gives the
   reference's misfit) differentiates through it.
+* :func:`misfit_gradients` runs the misfits and gradients of many solves
+  together, their segments interleaved on one CUDA stream per solve.
 * :func:`ice_table21` builds that table differentiably from per-grain c-axis
   angles (colatitude theta, azimuth phi; R = Rz(phi) Ry(theta), the
   convention of vendor/ringfwi/axisfield.py:37-65 and cof.axes_from_params),
@@ -63,26 +65,47 @@ class AdjointSolve:
 
     def forward(self, nt=None):
         """Traces (nt, n_groups) as a device tensor; keeps checkpoints."""
+        for _ in self.forward_segments(nt):
+            pass
+        self.solve.check_status()
+        return self.solve.traces[:self.nt, :self.solve.n_groups]
+
+    def forward_segments(self, nt=None):
+        """Generator form of :meth:`forward`: each iteration issues one
+        checkpoint segment on the current stream, without synchronising."""
         s = self.solve
         nt = s.nt if nt is None else int(nt)
         s.reset()
         self.ckpt = {}
+        self.nt = nt
         for a in range(0, nt, self.K):
             self.ckpt[a] = s.state.clone()
             s.run(a, min(a + self.K, nt))
-        self.nt = nt
-        s.check_status()
-        return s.traces[:nt, :s.n_groups]
+            yield a
 
     def backward(self, residual):
         """dJ/dC (n_mat, 21) float64 for the trace adjoint `residual`
         (nt, n_groups): for J = 0.5 ||traces - d||^2 it is traces - d."""
+        grad = None
+        for grad in self.backward_segments(residual):
+            pass
+        self.solve.check_status()
+        return grad.cpu().numpy()
+
+    def backward_segments(self, residual):
+        """Generator form of :meth:`backward`: allocates the adjoint state,
+        then each iteration issues the recompute and reverse sweep of one
+        segment (last first) on the current stream and yields the device
+        gradient accumulated so far ((n_mat, 21) float64)."""
         torch = self.torch
         s = self.solve
         nt, ng = self.nt, s.n_groups
         dev, tdt = s.device, s.tdt
         shape = s.shape
-        res = torch.as_tensor(np.asarray(residual), dtype=tdt).reshape(nt, ng).to(dev).contiguous()
+        if isinstance(residual, torch.Tensor):
+            res = residual.to(device=dev, dtype=tdt).reshape(nt, ng).contiguous()
+        else:
+            res = torch.as_tensor(np.asarray(residual), dtype=tdt).reshape(nt, ng).to(dev).contiguous()
         L = _bind()
         with torch.cuda.device(dev):
             lam = torch.zeros((9,) + shape, dtype=tdt, device=dev)
@@ -97,16 +120,71 @@ class AdjointSolve:
         adj.scratch = scratch.data_ptr()
         adj.grad = grad.data_ptr()
         stream = torch.cuda.current_stream(dev)
-        starts = sorted(self.ckpt)
-        for a in reversed(starts):
+        for a in reversed(sorted(self.ckpt)):
             b = min(a + self.K, nt)
             s.state.copy_(self.ckpt[a])
             # recompute the segment and step back through it in one C call
             with torch.cuda.device(dev):
                 _capi.check(L.pe_solver_adjoint_segment(s._h, C.byref(s._st), C.byref(adj), hist.data_ptr(),
                                                         a, b, res.data_ptr(), C.c_void_p(stream.cuda_stream)))
-        s.check_status()
-        return grad.cpu().numpy()
+            yield grad
+
+
+def misfit_gradients(problems, c21s, dobs):
+    """J_i = 0.5 ||traces_i(c21_i) - dobs_i||^2 and dJ_i/dc21_i for many
+    problems at once (a sweep's azimuths, an inversion's specimens): the
+    checkpoint segments of every solve, forward then reverse, are issued
+    round-robin on one CUDA stream per solve, so that solves too small to
+    fill the GPU run side by side. Per solve the same kernels run in the same
+    order as in the one-at-a-time gradient; only the order of the gradient's
+    atomic float64 sums may differ. Returns a list of (J, grad (n_mat_i, 21)
+    float64 numpy)."""
+    torch = _torch()
+    if not (len(problems) == len(c21s) == len(dobs)):
+        raise ValueError("one table and one observed record per problem")
+    adjs = []
+    try:
+        for p, c in zip(problems, c21s):
+            adjs.append(p.make_adjoint(np.asarray(c, float)))
+        streams = [torch.cuda.Stream(device=a.solve.device) for a in adjs]
+        for st, a in zip(streams, adjs):
+            st.wait_stream(torch.cuda.current_stream(a.solve.device))
+
+        def interleave(jobs):
+            live = list(jobs)
+            while live:
+                nxt = []
+                for st, g in live:
+                    with torch.cuda.stream(st):
+                        if next(g, None) is not None:
+                            nxt.append((st, g))
+                live = nxt
+
+        interleave([(st, a.forward_segments()) for st, a in zip(streams, adjs)])
+        res, J = [], []
+        for st, a, d in zip(streams, adjs, dobs):
+            with torch.cuda.stream(st):
+                tr = a.solve.traces[:a.nt, :a.solve.n_groups].to(torch.float64)
+                r = tr - torch.as_tensor(np.asarray(d, float), device=tr.device).reshape(tr.shape)
+                res.append(r)
+                J.append(0.5 * (r * r).sum())
+        grads = [None] * len(adjs)
+
+        def reverse(k, a, r):
+            for g in a.backward_segments(r):
+                grads[k] = g
+                yield True
+
+        interleave([(st, reverse(k, a, r)) for k, (st, a, r) in enumerate(zip(streams, adjs, res))])
+        out = []
+        for st, a, j, g in zip(streams, adjs, J, grads):
+            st.synchronize()
+            a.solve.check_status()
+            out.append((float(j.cpu()), g.cpu().numpy()))
+        return out
+    finally:
+        for a in adjs:
+            a.solve.close()
 
 
 # ---------------------------------------------------------------- autograd

@@ -155,3 +155,29 @@ def test_matches_reference_ringfwi_gradient():
     ours = np.concatenate([th.grad.numpy(), ph.grad.numpy()])
     ref = np.concatenate([g["g_theta"], g["g_phi"]])
     assert np.linalg.norm(ours - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_misfit_gradients_batched_equal_one_at_a_time(dtype):
+    """Several solves of different grids, their segments interleaved on one
+    stream each: every misfit and gradient equals its own one-at-a-time
+    autograd result (to the rounding of the gradient's atomic sums)."""
+    import torch
+    from pefdtd.adjoint import misfit_gradients
+    probs, c21s, dobs = [], [], []
+    for k, shape in enumerate([(18, 22, 24), (20, 24, 28), (16, 20, 22), (18, 22, 24)]):
+        p = make_small(nt=60, shape=shape, n_grains=4 + k, sponge=3, seed=30 + k)
+        prob = _problem(p, dtype=dtype, K=9 + k)
+        c0 = torch.tensor(_c21_of(p))
+        with torch.no_grad():
+            dobs.append(prob.traces(c0 * 1.01).numpy())
+        probs.append(prob)
+        c21s.append(c0.numpy())
+    got = misfit_gradients(probs, c21s, dobs)
+    for prob, c0, d, (J, g) in zip(probs, c21s, dobs, got):
+        c = torch.tensor(c0, requires_grad=True)
+        Jr = _loss(prob, c, torch.tensor(d))
+        Jr.backward()
+        gr = c.grad.numpy()
+        assert abs(J - float(Jr)) <= 1e-12 * abs(float(Jr))
+        assert np.abs(g - gr).max() <= 1e-10 * np.abs(gr).max()
