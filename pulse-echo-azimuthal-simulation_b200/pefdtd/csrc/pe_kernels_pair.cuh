@@ -287,6 +287,26 @@ struct PairPhases {
     int v, s;   // v loads / cell-box loads issued (and waited) so far
 };
 
+// Row of the strain tile a stress thread computes. Warps 0..6 take rows
+// 1..14 (the updated rows), two each; warp 7 takes the halo rows 0 and 15,
+// whose strains are only read by neighbours, so it skips the update phase
+// as a whole instead of leaving half of two warps idle there.
+static_assert(PS_N == 256 && PS_ROWS == 16, "pair_row assumes 8 warps of two 16-lane rows");
+__device__ __forceinline__ int pair_row(int tid)
+{
+    const int w = tid >> 5, h = (tid >> 4) & 1;
+    return w < 7 ? 2 * w + 1 + h : (h ? PS_ROWS - 1 : 0);
+}
+
+// Every x / y tap of strain tile (bx, by) lies inside the grid (then no x or
+// y guard can bind: every tap limit is at least T_H and every neighbour
+// exists).
+__device__ __forceinline__ bool pair_tile_inside(const StepArgs<float> &A, int bx, int by)
+{
+    const int S0 = bx * PS_OX - 2, S0y = by * PS_OY - 1;
+    return S0 - T_H >= 0 && S0 + PS_GW - 1 + T_H < A.nx && S0y - T_H >= 0 && S0y + PS_ROWS - 1 + T_H < A.ny;
+}
+
 // One z-march of a block over strain tile (bx, by), updating planes
 // [zb, ze). tab: the (n_mat, 36) table (shared memory when TS). Pipeline per
 // iteration (strain plane q, update plane z = q - 1):
@@ -295,8 +315,9 @@ struct PairPhases {
 // Every warp waits on the mbarriers itself. One v slot suffices (its refill
 // overlaps the update phase); the cell boxes alternate between two slots and
 // are issued a plane ahead. The caller synchronises the block before a march
-// that follows another.
-template <int NC, bool TS>
+// that follows another. TIN: pair_tile_inside(A, bx, by) holds, and the
+// x / y limits and guards are compile-time constants.
+template <int NC, bool TS, bool TIN>
 __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, const StepArgs<float> &A,
                                                   const float *tab, unsigned char *smem, int bx, int by,
                                                   int zb, int ze, PairPhases &ph)
@@ -307,12 +328,12 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     float *gs = sslots + 2 * PS_SSLOT;
     const int tid = threadIdx.x;
     (void)tab;
-    const int l = tid & (PR_LX - 1), r = tid >> 4;
+    const int l = tid & (PR_LX - 1), r = pair_row(tid);
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const long long sy = A.sy, sz = A.sz;
     const int S0 = bx * PS_OX - 2, S0y = by * PS_OY - 1;   // first strain column / row (S0 even)
     const int gx0 = S0 + 2 * l, gy = S0y + r;
-    const bool pair_ok = gx0 >= 0 && gx0 < nx && gy >= 0 && gy < ny;   // nx even: both columns
+    const bool pair_ok = TIN || (gx0 >= 0 && gx0 < nx && gy >= 0 && gy < ny);   // nx even: both columns
     const int col = pair_ok ? (int)(gy * sy + gx0) : 0;
     const long long n = *A.step + A.k;
     const float wn = A.n_src ? A.wavelet[n] : 0.f;
@@ -354,23 +375,28 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     }
     TapLimits tl;
     MoveGuards mg;
+    if constexpr (TIN) {
+        tl.xb[0] = tl.xb[1] = tl.xf[0] = tl.xf[1] = tl.yb = tl.yf = T_H;
+        mg.xlo[0] = mg.xlo[1] = mg.xhi[0] = mg.xhi[1] = mg.ylo = mg.yhi = true;
+    } else {
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        const int x = gx0 + c;
-        tl.xb[c] = lim_b(x, nx);
-        tl.xf[c] = lim_f(x, nx);
-        mg.xlo[c] = x >= 1;
-        mg.xhi[c] = x <= nx - 2;
+        for (int c = 0; c < 2; ++c) {
+            const int x = gx0 + c;
+            tl.xb[c] = lim_b(x, nx);
+            tl.xf[c] = lim_f(x, nx);
+            mg.xlo[c] = x >= 1;
+            mg.xhi[c] = x <= nx - 2;
+        }
+        tl.yb = lim_b(gy, ny);
+        tl.yf = lim_f(gy, ny);
+        mg.ylo = gy >= 1;
+        mg.yhi = gy <= ny - 2;
     }
-    tl.yb = lim_b(gy, ny);
-    tl.yf = lim_f(gy, ny);
-    mg.ylo = gy >= 1;
-    mg.yhi = gy <= ny - 2;
     // updated cells: inner 30 x 14 of the strain tile, inside the grid
-    const bool row_out = r >= 1 && r <= PS_OY && gy < ny;
+    const bool row_out = r >= 1 && r <= PS_OY && (TIN || gy < ny);
     bool out_c[2];
-    out_c[0] = row_out && l >= 1 && gx0 >= 0 && gx0 < nx;
-    out_c[1] = row_out && l <= PR_LX - 2 && gx0 + 1 >= 0 && gx0 + 1 < nx;
+    out_c[0] = row_out && l >= 1 && (TIN || (gx0 >= 0 && gx0 < nx));
+    out_c[1] = row_out && l <= PR_LX - 2 && (TIN || (gx0 + 1 >= 0 && gx0 + 1 < nx));
     const bool any_out = out_c[0] || out_c[1];
     float dyx = 1.0f, dxx[2] = {1.0f, 1.0f};
     if (A.dz && any_out) {
@@ -378,11 +404,10 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         dxx[0] = A.dx[gx0];
         dxx[1] = A.dx[gx0 + 1];
     }
-    const bool tile_in = S0 - T_H >= 0 && S0 + PS_GW - 1 + T_H < nx && S0y - T_H >= 0 &&
-                         S0y + PS_ROWS - 1 + T_H < ny;
     // a warp's two rows both past the last grid row: no strain of theirs is
-    // read by an updated cell, so the warp skips the strain work (warp-uniform)
-    const bool warp_rows_in = S0y + 2 * (tid >> 5) < ny;
+    // read by an updated cell, so the warp skips the strain work (warp-uniform;
+    // the lower of the warp's rows is pair_row of its first thread)
+    const bool warp_rows_in = TIN || S0y + pair_row(tid & ~31) < ny;
     const int cv = (r + T_H) * PS_VW + (S0 - xv) + 2 * l;   // cell 0 in a v box (even)
     const int cs = (r - 1) * PS_SW + (S0 - xs) + 2 * l;     // cell 0 in a cell box (even)
     const int cg = PS_GOFF + r * PS_GW + 2 * l;              // cell 0 in a strain plane
@@ -407,7 +432,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         const int z = q - 1;
         const uint32_t lab2 = lab_next;
         lab_next = ldlab(q);
-        const bool fast = NC == 4 && tile_in && q >= T_H && q <= nz - 1 - T_H;
+        const bool fast = NC == 4 && TIN && q >= T_H && q <= nz - 1 - T_H;
         if (warp_rows_in) {
             const float *tv = vslot + cv;
             float g[2][6];
@@ -553,10 +578,12 @@ __global__ void __launch_bounds__(PS_N, 2) k_stress_pair(const __grid_constant__
     stress_pair_init(smem_pair);
     if (TS) stage_table(tsm, tab36, n_mat);
     __syncthreads();
-    const int zb = blockIdx.z * A.zc;
+    const int zb = blockIdx.z * A.zc, ze = min(zb + A.zc, A.nz);
     PairPhases ph{0, 0};
-    stress_pair_march<NC, TS>(M, A, TS ? tsm : tab36, smem_pair, blockIdx.x, blockIdx.y, zb,
-                              min(zb + A.zc, A.nz), ph);
+    if (pair_tile_inside(A, blockIdx.x, blockIdx.y))
+        stress_pair_march<NC, TS, true>(M, A, TS ? tsm : tab36, smem_pair, blockIdx.x, blockIdx.y, zb, ze, ph);
+    else
+        stress_pair_march<NC, TS, false>(M, A, TS ? tsm : tab36, smem_pair, blockIdx.x, blockIdx.y, zb, ze, ph);
 }
 
 // ====================================================================== velocity
@@ -826,9 +853,12 @@ __global__ void __launch_bounds__(PS_N, 2)
             if (TS) stage_table(tsm, tabs[w.solve], n_mats[w.solve]);
         }
         __syncthreads();
-        const int zb = w.bz * As.zc;
-        stress_pair_march<NC, TS>(maps[w.solve], As, TS ? tsm : tabs[w.solve], smem_pair, w.bx, w.by, zb,
-                                  min(zb + As.zc, As.nz), ph);
+        const int zb = w.bz * As.zc, ze = min(zb + As.zc, As.nz);
+        const float *tab = TS ? tsm : tabs[w.solve];
+        if (pair_tile_inside(As, w.bx, w.by))
+            stress_pair_march<NC, TS, true>(maps[w.solve], As, tab, smem_pair, w.bx, w.by, zb, ze, ph);
+        else
+            stress_pair_march<NC, TS, false>(maps[w.solve], As, tab, smem_pair, w.bx, w.by, zb, ze, ph);
         cur = w.solve;
     }
 }
