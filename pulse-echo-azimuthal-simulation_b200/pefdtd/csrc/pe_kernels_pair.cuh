@@ -633,9 +633,18 @@ __device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, c
     }
 }
 
+// Every x / y tap of velocity tile (bx, by), and every face-density
+// neighbour, lies inside the grid.
+__device__ __forceinline__ bool pair_vtile_inside(const StepArgs<float> &A, int bx, int by)
+{
+    const int x0 = bx * PV_OX, y0 = by * PV_OY;
+    return x0 - T_H >= 0 && x0 + PV_OX - 1 + T_H < A.nx && y0 - T_H >= 0 && y0 + PV_OY - 1 + T_H < A.ny;
+}
+
 // One z-march of a block over cell tile (bx, by), planes [zb, ze); it0 as
-// in stress_pair_march.
-template <int NC>
+// in stress_pair_march. TIN: pair_vtile_inside(A, bx, by) holds, and the
+// x / y limits and neighbour tests are compile-time constants.
+template <int NC, bool TIN>
 __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, const StepArgs<float> &A,
                                                    const float *rho_tab, unsigned char *smem, int bx,
                                                    int by, int zb, int ze, int it0)
@@ -648,7 +657,7 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
     const long long sy = A.sy, sz = A.sz;
     const int x0 = bx * PV_OX, y0 = by * PV_OY;
     const int ix = x0 + 2 * l, iy = y0 + r;
-    const bool out_ok = ix < nx && iy < ny;   // nx even: both cells
+    const bool out_ok = TIN || (ix < nx && iy < ny);   // nx even: both cells
     const int col = out_ok ? (int)(iy * sy + ix) : 0;
     const bool has_dvol = A.dvol != nullptr;
     const unsigned bytes = (5u * PV_TSZ + 3u * PV_CSZ + (has_dvol ? (unsigned)PV_CSZ : 0u)) * 4u;
@@ -680,23 +689,25 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
         r5[0][k] = c.x; r5[1][k] = c.y;
     }
     TapLimits tl;
+    if constexpr (TIN) {
+        tl.xb[0] = tl.xb[1] = tl.xf[0] = tl.xf[1] = tl.yb = tl.yf = T_H;
+    } else {
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        tl.xb[c] = lim_b(ix + c, nx);
-        tl.xf[c] = lim_f(ix + c, nx);
+        for (int c = 0; c < 2; ++c) {
+            tl.xb[c] = lim_b(ix + c, nx);
+            tl.xf[c] = lim_f(ix + c, nx);
+        }
+        tl.yb = lim_b(iy, ny);
+        tl.yf = lim_f(iy, ny);
     }
-    tl.yb = lim_b(iy, ny);
-    tl.yf = lim_f(iy, ny);
-    const bool xin1 = ix + 1 < nx - 1;   // cell 1 has a +x neighbour (cell 0 always does)
-    const bool yin = iy < ny - 1;
+    const bool xin1 = TIN || ix + 1 < nx - 1;   // cell 1 has a +x neighbour (cell 0 always does)
+    const bool yin = TIN || iy < ny - 1;
     float dyx = 1.0f, dxx[2] = {1.0f, 1.0f};
     if (A.dz && out_ok) {
         dyx = A.dy[iy];
         dxx[0] = A.dx[ix];
         dxx[1] = A.dx[ix + 1];
     }
-    const bool tile_in = x0 - T_H >= 0 && x0 + PV_OX - 1 + T_H < nx && y0 - T_H >= 0 &&
-                         y0 + PV_OY - 1 + T_H < ny;
     const int tc = (r + T_H) * PV_TW + 2 * l + T_H;
     const int cc = r * PV_OX + 2 * l;
     const uint32_t *lab32 = reinterpret_cast<const uint32_t *>(A.lab);
@@ -731,7 +742,7 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
         const float *slot = slots + sl * PV_SLOT;
         const float *t = slot + tc;
         float ax[2], ay[2], az[2];
-        const bool fast = NC == 4 && tile_in && z >= T_H && z <= nz - 1 - T_H;
+        const bool fast = NC == 4 && TIN && z >= T_H && z <= nz - 1 - T_H;
         if (fast) pair_vel_taps<NC, false>(A, z, t, t + PV_TSZ, t + 2 * PV_TSZ, t + 3 * PV_TSZ, t + 4 * PV_TSZ, r3, r4, r5, tl, ax, ay, az);
         else pair_vel_taps<NC, true>(A, z, t, t + PV_TSZ, t + 2 * PV_TSZ, t + 3 * PV_TSZ, t + 4 * PV_TSZ, r3, r4, r5, tl, ax, ay, az);
         if (out_ok) {
@@ -819,8 +830,11 @@ __global__ void __launch_bounds__(PV_N, 2) k_velocity_pair(const __grid_constant
         for (int i = tid; i < n_mat; i += PV_N) rsm[i] = A.rho[i];
     __syncthreads();
     const float *rho_tab = rho_smem ? rsm : A.rho;
-    const int zb = blockIdx.z * A.zc;
-    velocity_pair_march<NC>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, min(zb + A.zc, A.nz), 0);
+    const int zb = blockIdx.z * A.zc, ze = min(zb + A.zc, A.nz);
+    if (pair_vtile_inside(A, blockIdx.x, blockIdx.y))
+        velocity_pair_march<NC, true>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, ze, 0);
+    else
+        velocity_pair_march<NC, false>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, ze, 0);
 }
 
 // ---------------------------------------------------------------- batches
@@ -889,9 +903,11 @@ __global__ void __launch_bounds__(PV_N, 2)
             for (int i = threadIdx.x; i < n_mats[w.solve]; i += PV_N) rsm[i] = As.rho[i];
         }
         __syncthreads();
-        const int zb = w.bz * As.zc;
-        it0 += velocity_pair_march<NC>(maps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, min(zb + As.zc, As.nz),
-                                       it0);
+        const int zb = w.bz * As.zc, ze = min(zb + As.zc, As.nz);
+        if (pair_vtile_inside(As, w.bx, w.by))
+            it0 += velocity_pair_march<NC, true>(maps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, ze, it0);
+        else
+            it0 += velocity_pair_march<NC, false>(maps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, ze, it0);
         cur = w.solve;
     }
 }
