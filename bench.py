@@ -455,8 +455,9 @@ def main():
     tr = solve.traces_numpy(W + K)
     finite = bool(np.isfinite(tr).all())
 
-    # per-kernel split for the roofline (events around each launch)
-    solve.reset()
+    # per-kernel split for the roofline (events around each launch), taken
+    # from the state the timed steps left (a filled wavefield: the first steps
+    # after a reset skip most face-density divisions and run faster)
     ms_s, ms_v = solve.profile(min(50, K))
     solve.close()
     peak, peak_kind = _peaks()

@@ -42,6 +42,7 @@ struct StepArgs {
     const uint16_t *lab;     // material | flags
     const T *c21;            // (n_mat, C21_STRIDE)
     const T *rho;            // (n_mat,)
+    const float *rinv;       // (n_mat,) RN32(1 / rho) (FP32 solves), or null
     const float *dz, *dy, *dx;  // sponge tapers or null
     const float *dvol;          // damping volume or null
     int nz, ny, nx;

@@ -587,6 +587,64 @@ __global__ void __launch_bounds__(PS_N, 2) k_stress_pair(const __grid_constant__
 }
 
 // ====================================================================== velocity
+// a / b in float32 with IEEE round-to-nearest, for a face density b > 0 (the
+// reference divides, sim/core/fdtd.py:1237-1244). The float32 division's
+// slow path for tiny numerators (which fill a shell ahead of the wavefront)
+// otherwise costs a third of the velocity kernel. When b is the cell's own
+// density, y = RN32(1 / b) is at hand and Markstein's theorem gives the
+// correctly rounded quotient: with y within half an ulp of 1 / b and q1
+// within one ulp of a / b, r = a - b q1 is exact (one FMA) and RN(q1 + r y)
+// is RN(a / b), while nothing underflows (2^-100 <= |a| <= 2^100 here).
+// q1 comes from one correction of q0 = RN(a y) (which alone is only within
+// two ulps): q1 = RN(q0 + (a - b q0) y) is within half an ulp plus 2^-47
+// relative. Smaller numerators are scaled by 2^64 first (exact), and the
+// scaled quotient scaled back, which is exact while the result is a normal
+// float32 (|scaled quotient| >= 2^-62; the subnormal grid continues the
+// lowest binade's spacing, so the boundary itself is safe). A subnormal
+// result is |a| 2^149 / b rounded to an integer (ties to even) in units of
+// 2^-149: A = |a| 2^149 is an integer below 2^49, a candidate n comes from
+// the correctly rounded A / b, and the exact remainder A - b n (one FMA:
+// it is a multiple of ulp(b) below 2 b) moves n by at most one. Mixed-density
+// faces and non-finite or huge numerators divide in float64 and round once
+// more, which is exact (53 >= 2 * 24 + 2 bits, Figueroa's theorem; a
+// subnormal midpoint survives the float64 quotient unchanged). Zero
+// numerators return themselves (the sign of zero kept).
+__device__ __forceinline__ float markstein(float a, float b, float y)
+{
+    const float q0 = a * y;
+    const float q1 = fmaf(fmaf(-b, q0, a), y, q0);
+    return fmaf(fmaf(-b, q1, a), y, q1);
+}
+// 0 < |a| < 2^-100, y = RN32(1 / b)
+__device__ __forceinline__ float div_face_tiny(float a, float b, float y)
+{
+    const float qs = markstein(a * 0x1p64f, b, y);
+    if (fabsf(qs) >= 0x1p-62f) return qs * 0x1p-64f;
+    const float A = fabsf(a) * 0x1p100f * 0x1p49f;
+    float n = markstein(A, b, y);          // below 2^23 + 1: the result is subnormal
+    n = (n + 0x1p23f) - 0x1p23f;           // nearest integer, ties to even
+    const float R = fmaf(-b, n, A), hb = 0.5f * b;
+    const bool odd = (__float2int_rz(n) & 1) != 0;
+    if (R > hb || (R == hb && odd)) n += 1.0f;
+    else if (R < -hb || (R == -hb && odd)) n -= 1.0f;
+    return copysignf(n * 0x1p-100f * 0x1p-49f, a);
+}
+__device__ __forceinline__ float div_face_rcp(float a, float b, bool own, float y)
+{
+    const float aa = fabsf(a);
+    if (own && aa >= 0x1p-100f && aa <= 0x1p100f) return markstein(a, b, y);
+    if (a == 0.0f) return a;
+    if (own && aa < 0x1p-100f) return div_face_tiny(a, b, y);
+    return (float)((double)a / (double)b);
+}
+
+// reciprocal densities RN32(1 / rho), correctly rounded (IEEE division)
+__global__ void k_rho_inv(const float *rho, float *rinv, int n_mat)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < n_mat) rinv[m] = 1.0f / rho[m];
+}
+
 template <int NC, bool G>
 __device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, const float *t1,
                                               const float *t2, const float *t4, const float *t5,
@@ -773,13 +831,14 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
             for (int c = 0; c < 2; ++c) {
                 const bool xin = c == 0 ? true : xin1;
                 const float r0 = rho_tab[lc[c] & LAB_MAT];
+                const float y0 = __ldg(A.rinv + (lc[c] & LAB_MAT));
                 const float rvx = xin ? 0.5f * (r0 + rho_tab[lxv[c] & LAB_MAT]) : r0;
                 const float rvy = yin ? 0.5f * (r0 + rho_tab[lyv[c] & LAB_MAT]) : r0;
                 const float rvz = (z < nz - 1) ? 0.5f * (r0 + rho_tab[lzv[c] & LAB_MAT]) : r0;
                 float ux = A.dt_h * ax[c], uy = A.dt_h * ay[c], uz = A.dt_h * az[c];
-                ux = div_face(ux, rvx);
-                uy = div_face(uy, rvy);
-                uz = div_face(uz, rvz);
+                ux = div_face_rcp(ux, rvx, rvx == r0, y0);
+                uy = div_face_rcp(uy, rvy, rvy == r0, y0);
+                uz = div_face_rcp(uz, rvz, rvz == r0, y0);
                 vn[0][c] = (pick(vxo, c) + ux) * dmp[c];
                 vn[1][c] = (pick(vyo, c) + uy) * dmp[c];
                 vn[2][c] = (pick(vzo, c) + uz) * dmp[c];

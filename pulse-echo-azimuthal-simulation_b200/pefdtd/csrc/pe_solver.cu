@@ -103,6 +103,7 @@ struct PeSolver {
     pe::TmapsVelocity mv{};
     // FP32 pair-column kernels (the default where the grid allows them)
     float *tab36 = nullptr;     // (n_mat, 36) column-split stiffness
+    float *rinv = nullptr;      // (n_mat,) reciprocal densities (FP32 pair velocity kernel)
     bool pair_capable = false;  // FP32, rows of 16-byte multiples, maps encodable, smem fits
     bool pair = false;          // pair kernels in use for the current state
     bool solo = false;          // in a batch: fills the GPU alone, so runs its own launches
@@ -117,7 +118,7 @@ struct PeSolver {
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
         void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
-                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group, tab36};
+                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group, tab36, rinv};
         for (void *b : bufs)
             if (b) cudaFree(b);
     }
@@ -134,6 +135,7 @@ pe::StepArgs<T> make_args(const PeSolver *S, const PeState *st, int k)
     A.lab = S->lab;
     A.c21 = (const T *)S->c21;
     A.rho = (const T *)S->rho;
+    A.rinv = S->rinv;
     A.dz = S->dz;
     A.dy = S->dy;
     A.dx = S->dx;
@@ -623,6 +625,8 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
         if (c.dtype == PE_F32) {
             if ((rc = dev_alloc(&S->tab36, sizeof(float) * pe::TAB36 * c.n_mat))) return rc;
             pe::k_c21_to_tab36<<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)S->c21, S->tab36, c.n_mat);
+            if ((rc = dev_alloc(&S->rinv, sizeof(float) * c.n_mat))) return rc;
+            pe::k_rho_inv<<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)S->rho, S->rinv, c.n_mat);
         }
         PE_CUDA(cudaStreamSynchronize(st));
         cudaFree(c36);
