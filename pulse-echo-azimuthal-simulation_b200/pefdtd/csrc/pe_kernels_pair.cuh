@@ -826,22 +826,43 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
                 }
             }
             const float2 vxo = lds2(vc), vyo = lds2(vc + PV_CSZ), vzo = lds2(vc + 2 * PV_CSZ);
-            float vn[3][2];
+            // the six face divisions: Markstein quotients for all of them
+            // (independent chains), then the exact fallback for the lanes
+            // whose numerator or face rules that out (div_face_rcp)
+            float u[2][3], rv[2][3], yr[2], q[2][3];
+            bool fine = true;
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const bool xin = c == 0 ? true : xin1;
                 const float r0 = rho_tab[lc[c] & LAB_MAT];
-                const float y0 = __ldg(A.rinv + (lc[c] & LAB_MAT));
-                const float rvx = xin ? 0.5f * (r0 + rho_tab[lxv[c] & LAB_MAT]) : r0;
-                const float rvy = yin ? 0.5f * (r0 + rho_tab[lyv[c] & LAB_MAT]) : r0;
-                const float rvz = (z < nz - 1) ? 0.5f * (r0 + rho_tab[lzv[c] & LAB_MAT]) : r0;
-                float ux = A.dt_h * ax[c], uy = A.dt_h * ay[c], uz = A.dt_h * az[c];
-                ux = div_face_rcp(ux, rvx, rvx == r0, y0);
-                uy = div_face_rcp(uy, rvy, rvy == r0, y0);
-                uz = div_face_rcp(uz, rvz, rvz == r0, y0);
-                vn[0][c] = (pick(vxo, c) + ux) * dmp[c];
-                vn[1][c] = (pick(vyo, c) + uy) * dmp[c];
-                vn[2][c] = (pick(vzo, c) + uz) * dmp[c];
+                yr[c] = __ldg(A.rinv + (lc[c] & LAB_MAT));
+                rv[c][0] = xin ? 0.5f * (r0 + rho_tab[lxv[c] & LAB_MAT]) : r0;
+                rv[c][1] = yin ? 0.5f * (r0 + rho_tab[lyv[c] & LAB_MAT]) : r0;
+                rv[c][2] = (z < nz - 1) ? 0.5f * (r0 + rho_tab[lzv[c] & LAB_MAT]) : r0;
+                u[c][0] = A.dt_h * ax[c];
+                u[c][1] = A.dt_h * ay[c];
+                u[c][2] = A.dt_h * az[c];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    q[c][d] = markstein(u[c][d], rv[c][d], yr[c]);
+                    const float au = fabsf(u[c][d]);
+                    fine = fine && rv[c][d] == r0 && au >= 0x1p-100f && au <= 0x1p100f;
+                }
+            }
+            if (!fine) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float r0 = rho_tab[lc[c] & LAB_MAT];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) q[c][d] = div_face_rcp(u[c][d], rv[c][d], rv[c][d] == r0, yr[c]);
+                }
+            }
+            float vn[3][2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                vn[0][c] = (pick(vxo, c) + q[c][0]) * dmp[c];
+                vn[1][c] = (pick(vyo, c) + q[c][1]) * dmp[c];
+                vn[2][c] = (pick(vzo, c) + q[c][2]) * dmp[c];
             }
             const long long idx = (long long)z * sz + col;
             stg2(A.v[0] + idx, vn[0][0], vn[0][1]);
