@@ -23,7 +23,7 @@
 // order-2, cell-density, undamped vendor/ringfwi/elastic3d.py:348-463; this
 // one is the adjoint of the full production scheme.
 #pragma once
-#include "pe_kernels.cuh"
+#include "pe_kernels_pair.cuh"
 
 namespace pe {
 
@@ -39,6 +39,7 @@ struct AdjArgs {
     const uint16_t *lab;
     const T *c21;      // (n_mat, C21_STRIDE)
     const T *rho;
+    const float *rinv;  // (n_mat,) RN32(1 / rho) (FP32 solves), or null
     const float *dz, *dy, *dx, *dvol;
     int nz, ny, nx;
     long long sy, sz;
@@ -128,6 +129,20 @@ __global__ void k_adj_inject(AdjArgs<T> A, const long long *cells, const int *po
 }
 
 // ---------------------------------------------------------------- velocity transpose
+// a / b rounded as the division; in FP32 through the reciprocal table
+// (div_face_rcp: exact, without the float32 divide's slow path for the tiny
+// adjoint values ahead of the back-propagating front)
+template <typename T>
+__device__ __forceinline__ T adj_div(T a, T b, T r0, const float *rinv, int m)
+{
+    return a / b;
+}
+template <>
+__device__ __forceinline__ float adj_div<float>(float a, float b, float r0, const float *rinv, int m)
+{
+    return rinv ? div_face_rcp(a, b, b == r0, __ldg(rinv + m)) : a / b;
+}
+
 template <typename T>
 __global__ void k_adj_vel_u(AdjArgs<T> A)
 {
@@ -135,14 +150,15 @@ __global__ void k_adj_vel_u(AdjArgs<T> A)
     if (i >= (long long)A.nz * A.ny * A.nx) return;
     int iz, iy, ix;
     cell_of(A, i, iz, iy, ix);
-    const T r0 = A.rho[A.lab[i] & LAB_MAT];
+    const int m0 = A.lab[i] & LAB_MAT;
+    const T r0 = A.rho[m0];
     const T rvx = ix < A.nx - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + 1] & LAB_MAT]) : r0;
     const T rvy = iy < A.ny - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + A.sy] & LAB_MAT]) : r0;
     const T rvz = iz < A.nz - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + A.sz] & LAB_MAT]) : r0;
     const T s = (T)adj_damp(A, iz, iy, ix, i) * A.dt_h;
-    A.u[0][i] = s * A.lv[0][i] / rvx;
-    A.u[1][i] = s * A.lv[1][i] / rvy;
-    A.u[2][i] = s * A.lv[2][i] / rvz;
+    A.u[0][i] = adj_div(s * A.lv[0][i], rvx, r0, A.rinv, m0);
+    A.u[1][i] = adj_div(s * A.lv[1][i], rvy, r0, A.rinv, m0);
+    A.u[2][i] = adj_div(s * A.lv[2][i], rvz, r0, A.rinv, m0);
 }
 
 template <typename T>

@@ -782,6 +782,7 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
     A.lab = S->lab;
     A.c21 = (const T *)S->c21;
     A.rho = (const T *)S->rho;
+    A.rinv = S->rinv;
     A.dz = S->dz;
     A.dy = S->dy;
     A.dx = S->dx;
