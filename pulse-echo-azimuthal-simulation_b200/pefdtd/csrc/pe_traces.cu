@@ -22,7 +22,9 @@
 // computed on the host exactly as the reference's Python computes them.
 #include <cmath>
 #include <cstdint>
+#include <algorithm>
 #include <initializer_list>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -283,28 +285,52 @@ __global__ void __launch_bounds__(RED_T) k_analyse(const T *__restrict__ x, cons
     out[4 * tr + 3] = have_tail ? mx / (E1 > 1e-30 ? E1 : 1e-30) : NAN;
 }
 
-// Device copy of small host arrays, freed by the destructor after the
-// stream has been synchronised.
-struct Staged {
+// Device copies of a call's small host arrays (offsets, windows, time
+// steps) go to one grow-only buffer per device, held (mutex) for the whole
+// call: every entry point synchronises its stream before returning, so the
+// next call may reuse the buffer, and after the first calls on a device no
+// call allocates or frees device memory (cudaFree would also synchronise
+// the device).
+struct StageArea {
+    std::mutex mu;
     char *p = nullptr;
-    ~Staged() { if (p) cudaFree(p); }
+    size_t cap = 0;
+};
+constexpr int STAGE_DEVICES = 64;
+
+struct Staged {
+    std::unique_lock<std::mutex> lock;
 };
 
 cudaError_t stage(Staged &s, cudaStream_t st, std::initializer_list<std::pair<const void *, size_t>> parts,
                   std::vector<void *> &dst)
 {
+    static StageArea areas[STAGE_DEVICES];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= STAGE_DEVICES) return cudaErrorInvalidDevice;
+    StageArea &a = areas[dev];
+    s.lock = std::unique_lock<std::mutex>(a.mu);
     size_t total = 0;
     for (auto &q : parts) total += (q.second + 255) & ~size_t(255);
-    cudaError_t e = cudaMalloc(&s.p, total ? total : 256);
-    if (e != cudaSuccess) {
-        s.p = nullptr;
-        return e;
+    if (total > a.cap) {
+        if (a.p) cudaFree(a.p);
+        a.p = nullptr;
+        a.cap = 0;
+        const size_t want = std::max(total, std::max(a.cap * 2, (size_t)1 << 16));
+        e = cudaMalloc(&a.p, want);
+        if (e != cudaSuccess) {
+            a.p = nullptr;
+            return e;
+        }
+        a.cap = want;
     }
     size_t at = 0;
     for (auto &q : parts) {
-        dst.push_back(s.p + at);
+        dst.push_back(a.p + at);
         if (q.second) {
-            e = cudaMemcpyAsync(s.p + at, q.first, q.second, cudaMemcpyHostToDevice, st);
+            e = cudaMemcpyAsync(a.p + at, q.first, q.second, cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) return e;
         }
         at += (q.second + 255) & ~size_t(255);
