@@ -310,9 +310,10 @@ __device__ __forceinline__ bool pair_tile_inside(const StepArgs<float> &A, int b
 // One z-march of a block over strain tile (bx, by), updating planes
 // [zb, ze). tab: the (n_mat, 36) table (shared memory when TS). Pipeline per
 // iteration (strain plane q, update plane z = q - 1):
-//   wait v(q) | strains of q | block barrier | issue v(q + 1) and the cell
-//   boxes of z + 1 | wait cell boxes of z | updates of plane z
-// Every warp waits on the mbarriers itself. One v slot suffices (its refill
+//   wait v(q) | strains of q | (warp 7: wait cell boxes of z) | block
+//   barrier | issue v(q + 1) and the cell boxes of z + 1 | updates of plane z
+// Every warp waits on the v mbarrier itself; warp 7 (halo rows, nothing to
+// update) alone waits for the cell boxes. One v slot suffices (its refill
 // overlaps the update phase); the cell boxes alternate between two slots and
 // are issued a plane ahead. The caller synchronises the block before a march
 // that follows another. TIN: pair_tile_inside(A, bx, by) holds, and the
@@ -455,13 +456,16 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         rz[0][7] = nzv.x; rz[1][7] = nzv.y;
         ry[0][7] = nyv.x; ry[1][7] = nyv.y;
         rx[0][7] = nxv.x; rx[1][7] = nxv.y;
+        // the cell boxes of plane z (issued a plane earlier): warp 7, which
+        // has no cell to update, waits for them before the block barrier,
+        // and the barrier orders every other warp's reads after that wait
+        const int us = s0 + z - zb;   // cell-box load index of plane z
+        if ((tid >> 5) == 7 && z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
         __syncthreads();   // strains of q written; the v slot is free; the updates of z - 1 are done
         if (tid == 0) {
             if (q + 1 <= ze) issue_v(q + 1);
             if (q >= zb + 2 && q < ze) issue_s(q);   // plane z + 1, into the slot plane z - 1 used
         }
-        const int us = s0 + z - zb;   // cell-box load index of plane z
-        if (z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
         if (z >= zb && any_out) {
             // strain planes z - 1, z, z + 1 were written at iterations i - 2, i - 1, i
             const int zr3 = r3 == 0 ? 2 : r3 - 1;   // plane z modulo 3
