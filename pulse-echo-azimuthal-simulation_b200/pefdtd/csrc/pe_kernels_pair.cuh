@@ -462,7 +462,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         const int us = s0 + z - zb;   // cell-box load index of plane z
         if ((tid >> 5) == 7 && z >= zb) mbar_wait(bars + 1 + (us & 1), (unsigned)(us >> 1) & 1u, status);
         __syncthreads();   // strains of q written; the v slot is free; the updates of z - 1 are done
-        if (tid == 0) {
+        if (tid == 7 * 32) {   // warp 7: idle while the others update
             if (q + 1 <= ze) issue_v(q + 1);
             if (q >= zb + 2 && q < ze) issue_s(q);   // plane z + 1, into the slot plane z - 1 used
         }
