@@ -46,7 +46,9 @@ struct AdjArgs {
     T c[4];
     int nc;
     T inv_h, dt, dt_h;
-    double *grad;      // (n_mat, 21) dJ/dC, upper triangle row major
+    double *grad;      // (grad_rep, n_mat, 21) dJ/dC, upper triangle row major
+    int grad_rep;      // replicas of the table the atomic sums spread over (>= 1)
+    int n_mat;
 };
 
 __device__ __forceinline__ bool gF(int x, int j, int n) { return x >= j && x < n - j - 1; }
@@ -341,9 +343,16 @@ __global__ void k_adj_stress(AdjArgs<T> A)
     }
     // per-material gradient: one full-warp butterfly per distinct material in
     // the warp (lanes of other materials contribute zero), then one f64
-    // atomic per material and constant; every lane of the warp takes part
+    // atomic per material and constant; every lane of the warp takes part.
+    // Warps add into one of grad_rep replicas of the table (by warp index),
+    // so that the warps of a large single-material region (the couplant)
+    // do not all serialise on the same 21 addresses.
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    double *gtab = A.grad;
+    if (A.grad_rep > 1)
+        gtab += (long long)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)A.grad_rep) *
+                A.n_mat * 21;
     const int my = live ? m : -1;
     unsigned remaining = __ballot_sync(full, live);
     while (remaining) {
@@ -355,9 +364,22 @@ __global__ void k_adj_stress(AdjArgs<T> A)
             double v = my == mm ? gsum[k] : 0.0;
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(full, v, off);
-            if (lane == src) atomicAdd(A.grad + (long long)mm * 21 + k, v);
+            if (lane == src) atomicAdd(gtab + (long long)mm * 21 + k, v);
         }
     }
+}
+
+// grad += sum of the replicas, which are left zero
+__global__ void k_grad_fold(double *rep, int nrep, long long len, double *grad)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    double s = 0.0;
+    for (int r = 0; r < nrep; ++r) {
+        s += rep[(long long)r * len + i];
+        rep[(long long)r * len + i] = 0.0;
+    }
+    grad[i] += s;
 }
 
 template <typename T>

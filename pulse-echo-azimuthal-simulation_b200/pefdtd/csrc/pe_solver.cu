@@ -104,6 +104,8 @@ struct PeSolver {
     // FP32 pair-column kernels (the default where the grid allows them)
     float *tab36 = nullptr;     // (n_mat, 36) column-split stiffness
     float *rinv = nullptr;      // (n_mat,) reciprocal densities (FP32 pair velocity kernel)
+    double *grad_rep = nullptr; // (nrep, n_mat, 21) replicas the adjoint's gradient sums spread over
+    int nrep = 0;
     bool pair_capable = false;  // FP32, rows of 16-byte multiples, maps encodable, smem fits
     bool pair = false;          // pair kernels in use for the current state
     bool solo = false;          // in a batch: fills the GPU alone, so runs its own launches
@@ -118,7 +120,7 @@ struct PeSolver {
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
         void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
-                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group, tab36, rinv};
+                        rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group, tab36, rinv, grad_rep};
         for (void *b : bufs)
             if (b) cudaFree(b);
     }
@@ -762,8 +764,11 @@ int64_t pe_solver_launch_count(const PeSolver *S) { return S ? S->launches : -1;
 
 namespace {
 
+// grad: the table the step's gradient sums go to (adj->grad, or the
+// solver's replicas when nrep > 1)
 template <typename T>
-int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *residual, cudaStream_t st)
+int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *residual, cudaStream_t st,
+                   double *grad, int nrep)
 {
     const PeConfig &c = S->cfg;
     pe::AdjArgs<T> A{};
@@ -797,7 +802,9 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
     A.inv_h = (T)(1.0 / c.h);
     A.dt = (T)c.dt;
     A.dt_h = (T)(c.dt / c.h);
-    A.grad = adj->grad;
+    A.grad = grad;
+    A.grad_rep = nrep;
+    A.n_mat = c.n_mat;
     const unsigned nb = (unsigned)((ncell + 255) / 256);
     if (S->n_rec > 0 && residual) {
         const T *row = (const T *)residual + (size_t)n * S->n_groups;
@@ -829,8 +836,8 @@ int pe_solver_adjoint_step(PeSolver *S, const PeAdjoint *adj, int64_t n, const v
         if (!adj->ls[i]) return fail(PE_ERR_INVALID, "adjoint stress buffers missing");
     if (n < 0) return fail(PE_ERR_INVALID, "negative step");
     cudaStream_t st = (cudaStream_t)stream;
-    return S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, adj, n, residual, st)
-                                  : adjoint_step_t<float>(S, adj, n, residual, st);
+    return S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, adj, n, residual, st, adj->grad, 1)
+                                  : adjoint_step_t<float>(S, adj, n, residual, st, adj->grad, 1);
 }
 
 int pe_solver_adjoint_segment(PeSolver *S, const PeState *state, const PeAdjoint *adj0, void *v_hist,
@@ -866,14 +873,25 @@ int pe_solver_adjoint_segment(PeSolver *S, const PeState *state, const PeAdjoint
         }
     }
     PE_CUDA(cudaGetLastError());
-    // then the adjoint steps backwards through it
+    // then the adjoint steps backwards through it, the gradient sums spread
+    // over replicas of the table (allocated zero on the first segment, left
+    // zero by the fold)
+    const long long glen = (long long)S->cfg.n_mat * 21;
+    if (!S->grad_rep) {
+        const int nrep = (int)std::max(1LL, std::min(64LL, (64LL << 20) / (glen * 8)));
+        if ((rc = dev_alloc(&S->grad_rep, sizeof(double) * (size_t)(glen * nrep)))) return rc;
+        PE_CUDA(cudaMemsetAsync(S->grad_rep, 0, sizeof(double) * (size_t)(glen * nrep), st));
+        S->nrep = nrep;
+    }
     PeAdjoint adj = *adj0;
     for (int64_t n = b - 1; n >= a; --n) {
         for (int c = 0; c < 3; ++c) adj.v_prev[c] = hist + ((size_t)(n - a) * 3 + c) * fb;
-        rc = S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, &adj, n, residual, st)
-                                    : adjoint_step_t<float>(S, &adj, n, residual, st);
+        rc = S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, &adj, n, residual, st, S->grad_rep, S->nrep)
+                                    : adjoint_step_t<float>(S, &adj, n, residual, st, S->grad_rep, S->nrep);
         if (rc) return rc;
     }
+    pe::k_grad_fold<<<(unsigned)((glen + 255) / 256), 256, 0, st>>>(S->grad_rep, S->nrep, glen, adj0->grad);
+    PE_CUDA(cudaGetLastError());
     return PE_OK;
 }
 
