@@ -261,8 +261,10 @@ __global__ void k_adj_w(AdjArgs<T> A)
         }
 }
 
+constexpr int ADJ_STRESS_WARPS = 8;   // k_adj_stress runs 256-thread blocks
+
 template <typename T>
-__global__ void k_adj_stress(AdjArgs<T> A)
+__global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T> A)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < (long long)A.nz * A.ny * A.nx;
@@ -303,14 +305,16 @@ __global__ void k_adj_stress(AdjArgs<T> A)
                     q[p][J] = acc * T(0.25);
                 }
             }
-        // dJ/dC_IJ for I <= J: e_I q[p(I)][J] + e_J q[p(J)][I]  (I != J)
+        // dJ/dC_IJ for I <= J: e_I q[p(I)][J] + e_J q[p(J)][I]  (I != J),
+        // formed in the solve's precision (in FP32 one rounding of the
+        // cell's term, as its fields carry) and summed over cells in f64
 #pragma unroll
         for (int I = 0; I < 6; ++I)
 #pragma unroll
             for (int J = I; J < 6; ++J) {
-                double v = (double)e[I] * (double)q[VP[I]][J];
-                if (J != I) v += (double)e[J] * (double)q[VP[J]][I];
-                gsum[c21_slot(I, J)] = v;
+                T v = e[I] * q[VP[I]][J];
+                if (J != I) v += e[J] * q[VP[J]][I];
+                gsum[c21_slot(I, J)] = (double)v;
             }
         // strain adjoint t_J: direct term plus transposed moves of
         // W[p][J](x) = sum_{I at p} C_IJ(x) e_I(x) from the forward cells x
@@ -341,18 +345,20 @@ __global__ void k_adj_stress(AdjArgs<T> A)
 #pragma unroll
         for (int J = 0; J < 6; ++J) A.t[J][i] = tJ[J];
     }
-    // per-material gradient: one full-warp butterfly per distinct material in
-    // the warp (lanes of other materials contribute zero), then one f64
-    // atomic per material and constant; every lane of the warp takes part.
-    // Warps add into one of grad_rep replicas of the table (by warp index),
-    // so that the warps of a large single-material region (the couplant)
-    // do not all serialise on the same 21 addresses.
+    // per-material gradient, once per distinct material in the warp: every
+    // lane writes its 21 sums (zero for other materials) to the warp's
+    // 32 x 21 tile in shared memory, then lanes 0..20 each add up one column
+    // and issue the 21 f64 atomics together. Warps add into one of grad_rep
+    // replicas of the table (by warp index), so that the warps of a large
+    // single-material region (the couplant) do not all serialise on the same
+    // 21 addresses. Tile rows are 21 doubles apart: the row stores and the
+    // column loads are both free of bank conflicts.
+    __shared__ double red[ADJ_STRESS_WARPS][32][21];
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *gtab = A.grad;
     if (A.grad_rep > 1)
-        gtab += (long long)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)A.grad_rep) *
-                A.n_mat * 21;
+        gtab += (long long)((blockIdx.x * (blockDim.x >> 5) + warp) % (unsigned)A.grad_rep) * A.n_mat * 21;
     const int my = live ? m : -1;
     unsigned remaining = __ballot_sync(full, live);
     while (remaining) {
@@ -360,12 +366,20 @@ __global__ void k_adj_stress(AdjArgs<T> A)
         const int mm = __shfl_sync(full, my, src);
         remaining &= ~__ballot_sync(full, my == mm);
 #pragma unroll
-        for (int k = 0; k < 21; ++k) {
-            double v = my == mm ? gsum[k] : 0.0;
+        for (int k = 0; k < 21; ++k) red[warp][lane][k] = my == mm ? gsum[k] : 0.0;
+        __syncwarp();
+        if (lane < 21) {
+            double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;   // four chains, for latency
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(full, v, off);
-            if (lane == src) atomicAdd(gtab + (long long)mm * 21 + k, v);
+            for (int r = 0; r < 32; r += 4) {
+                v0 += red[warp][r][lane];
+                v1 += red[warp][r + 1][lane];
+                v2 += red[warp][r + 2][lane];
+                v3 += red[warp][r + 3][lane];
+            }
+            atomicAdd(gtab + (long long)mm * 21 + lane, (v0 + v1) + (v2 + v3));
         }
+        __syncwarp();
     }
 }
 
