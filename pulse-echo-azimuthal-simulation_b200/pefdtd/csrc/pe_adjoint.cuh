@@ -13,9 +13,9 @@
 //   k_adj_strain    g = D v^{n-1}                         (same taps as forward)
 //   k_adj_w         w[p][J] = sum over stresses I at position p of
 //                   C_IJ dt ls_I, for the 18 moved (p, J), once per cell
-//   k_adj_stress    dJ/dC[m] += dt ls (x) (M g); t = M^T C^T (dt ls)
+//   k_adj_stress    dJ/dC[m] += dt ls (x) (M g); t = M^T C^T (dt ls);
+//                   then ls = d ls
 //   k_adj_velfin    lv = d lv + D^T t
-//   k_adj_damp      ls = d ls
 // Every transpose is a gather that evaluates the forward guard at the forward
 // cell it reads from, so the boundaries transpose exactly and no result
 // depends on thread order except the per-material gradient sums (f64
@@ -344,6 +344,12 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
         }
 #pragma unroll
         for (int J = 0; J < 6; ++J) A.t[J][i] = tJ[J];
+        // the step's last use of ls at this cell (k_adj_w ran before, and
+        // only this thread reads it here): apply the deferred damping,
+        // ls = d ls (the transpose of the forward s^{n-1} * d)
+        const T d = (T)adj_damp(A, iz, iy, ix, i);
+#pragma unroll
+        for (int I = 0; I < 6; ++I) A.ls[I][i] = d * A.ls[I][i];
     }
     // per-material gradient, once per distinct material in the warp: every
     // lane writes its 21 sums (zero for other materials) to the warp's
@@ -420,18 +426,6 @@ __global__ void k_adj_velfin(AdjArgs<T> A)
     A.lv[0][i] = d * A.lv[0][i] + ih * gx;
     A.lv[1][i] = d * A.lv[1][i] + ih * gy;
     A.lv[2][i] = d * A.lv[2][i] + ih * gz;
-}
-
-template <typename T>
-__global__ void k_adj_damp(AdjArgs<T> A)
-{
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)A.nz * A.ny * A.nx) return;
-    int iz, iy, ix;
-    cell_of(A, i, iz, iy, ix);
-    const T d = (T)adj_damp(A, iz, iy, ix, i);
-#pragma unroll
-    for (int I = 0; I < 6; ++I) A.ls[I][i] = d * A.ls[I][i];
 }
 
 }  // namespace pe

@@ -818,7 +818,6 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
     pe::k_adj_w<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_stress<T><<<nb, 256, 0, st>>>(A);
     pe::k_adj_velfin<T><<<nb, 256, 0, st>>>(A);
-    pe::k_adj_damp<T><<<nb, 256, 0, st>>>(A);
     PE_CUDA(cudaGetLastError());
     return PE_OK;
 }
