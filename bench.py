@@ -36,6 +36,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -64,7 +65,10 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # PE_CLOCKS_DIR keeps the raw samples (e.g. to attach them to a run);
+        # by default they go to the system temporary directory
+        self.path = os.path.join(os.environ.get("PE_CLOCKS_DIR") or tempfile.gettempdir(),
+                                 f"pefdtd_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
