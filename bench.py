@@ -135,6 +135,34 @@ def _device_solve(p, nt_total):
     return solve
 
 
+def _fp64_check(p, nt, tr32):
+    """The FP32 run's traces against an FP64 run of the same kernels on the
+    same inputs (relative L2 and the Hilbert-envelope pick)."""
+    from pefdtd import wavelets
+    from pefdtd.damping import sponge_axis_profiles
+    from pefdtd.fdtd import DeviceSolve, _flat_probe
+    shape = p["lab"].shape
+    s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float64)
+    sv = DeviceSolve(p["mats"], p["Ct"], p["rho_t"], p["h"], p["dt"], p["coeffs"], s_idx, s_w, r_off, r_idx,
+                     r_w, record=p["record"], damped_record=True, sponge=sponge_axis_profiles(shape, p["sponge"]),
+                     dtype="float64")
+    try:
+        sv.set_wavelet(p["wavelet"][:nt])
+        sv.run(0, nt)
+        tr64 = sv.traces_numpy(nt)
+    finally:
+        sv.close()
+    a = np.asarray(tr32, float)[:nt, 0]
+    b = np.asarray(tr64, float)[:nt, 0]
+    rel = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    t = np.arange(nt) * p["dt"]
+    pa = wavelets.pick_peak(t, a, dt=p["dt"])
+    pb = wavelets.pick_peak(t, b, dt=p["dt"])
+    same = bool(pa[2] == pb[2] and (np.isnan(pa[0]) and np.isnan(pb[0])
+                                    or round(pa[0] / p["dt"]) == round(pb[0] / p["dt"])))
+    return {"steps": nt, "trace_rel_l2": rel, "pick_s_f32_f64": [pa[0], pb[0]], "pick_identical": same}
+
+
 def _e2e(p, steps, warm=True):
     """Same metric through the public C ABI host entry (pe_forward_host):
     pinned host labels/tables/probe in, traces out, all inside the timing
@@ -501,6 +529,8 @@ def main():
             "gpu_launches": launches, "traces_finite": finite}
     if rank == 0 and not args.no_e2e:
         line["e2e"] = _e2e(p, K)
+    if rank == 0 and not args.no_cpu:
+        line["fp64_check"] = _fp64_check(p, W + K, tr)
     clk_sum = clk.summary()
     if clk_sum is not None:
         line["clocks"] = clk_sum
