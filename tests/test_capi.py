@@ -59,3 +59,37 @@ def test_invalid_arguments_fail_cleanly_without_a_device():
     rc = L.pe_solver_create(C.byref(cfg), C.byref(md), C.byref(pr), C.byref(h))
     assert rc == _capi.PE_ERR_INVALID
     assert b"order <= 8" in L.pe_last_error()
+
+
+def test_trace_entry_points_reject_bad_arguments_without_a_device():
+    """pe_trace_*: empty batches, bad offsets, short windows and bad filter
+    sizes are refused before any device work (reference: the ValueErrors of
+    np.argmax on an empty window and of scipy's filtfilt)."""
+    from pefdtd import _capi
+    L = _capi.lib()
+    x = np.zeros(16, np.float32)
+    env = np.zeros(16, np.float64)
+    off = np.array([0, 16], np.int64)
+    bad_off = np.array([1, 16], np.int64)      # must start at 0
+    empty = np.array([0, 0], np.int64)          # an empty trace
+    p = lambda a: a.ctypes.data                 # noqa: E731
+    assert L.pe_trace_envelope(p(x), _capi.PE_F32, p(off), 0, p(env), None) == _capi.PE_ERR_INVALID
+    assert L.pe_trace_envelope(p(x), _capi.PE_F32, p(bad_off), 1, p(env), None) == _capi.PE_ERR_INVALID
+    assert L.pe_trace_envelope(p(x), _capi.PE_F32, p(empty), 1, p(env), None) == _capi.PE_ERR_INVALID
+    assert L.pe_trace_envelope(p(x), 7, p(off), 1, p(env), None) == _capi.PE_ERR_INVALID
+    b = np.ones(3)
+    a = np.ones(3)
+    zi = np.zeros(2)
+    # padlen must be below every trace's length, filters of 2..8 taps
+    assert L.pe_trace_detrend(p(x), _capi.PE_F32, p(off), 1, p(b), p(a), 3, p(zi), 16, p(env),
+                              None) == _capi.PE_ERR_INVALID
+    assert L.pe_trace_detrend(p(x), _capi.PE_F32, p(off), 1, p(b), p(a), 9, p(zi), 9, p(env),
+                              None) == _capi.PE_ERR_INVALID
+    win = np.array([4, 6], np.int64)            # hi must exceed lo + 2
+    dt = np.array([1e-8])
+    out = np.zeros(3)
+    assert L.pe_trace_pick(p(env), p(off), 1, p(win), p(dt), p(out), None) == _capi.PE_ERR_INVALID
+    win4 = np.array([5, 5, 0, 16], np.int64)    # empty E1 window
+    tf = np.array([1e-8, 1e8])
+    assert L.pe_trace_analyse(p(x), _capi.PE_F32, p(env), p(off), 1, p(win4), p(tf), p(out),
+                              None) == _capi.PE_ERR_INVALID
