@@ -365,8 +365,13 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
     double *gtab = A.grad;
     if (A.grad_rep > 1)
         gtab += (long long)((blockIdx.x * (blockDim.x >> 5) + warp) % (unsigned)A.grad_rep) * A.n_mat * 21;
+    // lanes whose 21 terms are all zero (no overlap of the adjoint stress
+    // and the forward strain at the cell) add nothing and sit out
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 21; ++k) any = any || gsum[k] != 0.0;
     const int my = live ? m : -1;
-    unsigned remaining = __ballot_sync(full, live);
+    unsigned remaining = __ballot_sync(full, live && any);
     while (remaining) {
         const int src = __ffs(remaining) - 1;
         const int mm = __shfl_sync(full, my, src);
