@@ -48,6 +48,7 @@ import numpy as np  # noqa: E402
 ALG_BYTES_STEP = 74      # 9 f32 fields read + written, u16 label read, per cell-update
 ALG_BYTES_STRESS = 62    # v read 12, s read 24 + write 24, label 2
 ALG_BYTES_VEL = 50       # s read 24, v read 12 + write 12, label 2
+SPLIT_FROM = 300         # the per-kernel split is taken from this step on (filled wavefield)
 
 
 def _peaks():
@@ -118,9 +119,21 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def _problem(workload, nt):
+def _problem(workload, nt, use_gpu=None):
     from pefdtd import workloads
-    return workloads.make_problem(workload, nt=nt)
+    return workloads.make_problem(workload, nt=nt, use_gpu=use_gpu)
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def _device_solve(p, nt_total):
@@ -135,32 +148,44 @@ def _device_solve(p, nt_total):
     return solve
 
 
-def _fp64_check(p, nt, tr32):
-    """The FP32 run's traces against an FP64 run of the same kernels on the
-    same inputs (relative L2 and the Hilbert-envelope pick)."""
-    from pefdtd import wavelets
+def _fp64_check(p, nt):
+    """The workload at its full length, FP32 against an FP64 run of the same
+    kernels on the same inputs: relative L2 of the traces, and the
+    Hilbert-envelope pick of the disk's bottom-face echo in both (searched
+    past the transmitted burst, required inside the echo window)."""
+    from pefdtd import wavelets, workloads
     from pefdtd.damping import sponge_axis_profiles
     from pefdtd.fdtd import DeviceSolve, _flat_probe
     shape = p["lab"].shape
-    s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float64)
-    sv = DeviceSolve(p["mats"], p["Ct"], p["rho_t"], p["h"], p["dt"], p["coeffs"], s_idx, s_w, r_off, r_idx,
-                     r_w, record=p["record"], damped_record=True, sponge=sponge_axis_profiles(shape, p["sponge"]),
-                     dtype="float64")
-    try:
-        sv.set_wavelet(p["wavelet"][:nt])
-        sv.run(0, nt)
-        tr64 = sv.traces_numpy(nt)
-    finally:
-        sv.close()
-    a = np.asarray(tr32, float)[:nt, 0]
-    b = np.asarray(tr64, float)[:nt, 0]
+    spec = p["spec"]
+    wav = wavelets.hann_tone_burst(nt, p["dt"], spec["f0"], n_cycles=spec["n_cycles"])
+    out = {}
+    for dtype, npdt in (("float32", np.float32), ("float64", np.float64)):
+        s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], npdt)
+        sv = DeviceSolve(p["mats"], p["Ct"], p["rho_t"], p["h"], p["dt"], p["coeffs"], s_idx, s_w, r_off,
+                         r_idx, r_w, record=p["record"], damped_record=True,
+                         sponge=sponge_axis_profiles(shape, p["sponge"]), dtype=dtype)
+        try:
+            sv.set_wavelet(wav)
+            sv.run(0, nt)
+            sv.check_status()
+            out[dtype] = np.asarray(sv.traces_numpy(nt), float)[:, 0]
+        finally:
+            sv.close()
+    a, b = out["float32"], out["float64"]
     rel = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
     t = np.arange(nt) * p["dt"]
-    pa = wavelets.pick_peak(t, a, dt=p["dt"])
-    pb = wavelets.pick_peak(t, b, dt=p["dt"])
-    same = bool(pa[2] == pb[2] and (np.isnan(pa[0]) and np.isnan(pb[0])
-                                    or round(pa[0] / p["dt"]) == round(pb[0] / p["dt"])))
-    return {"steps": nt, "trace_rel_l2": rel, "pick_s_f32_f64": [pa[0], pb[0]], "pick_identical": same}
+    t_lo, w_lo, w_hi = workloads.bottom_echo_window(p)
+    pa = wavelets.pick_peak(t, a, t_lo=t_lo, dt=p["dt"])
+    pb = wavelets.pick_peak(t, b, t_lo=t_lo, dt=p["dt"])
+    k_lo, k_hi = int(t_lo / p["dt"]), nt
+    same = bool(pa[2] == pb[2] and round(pa[0] / p["dt"]) == round(pb[0] / p["dt"]))
+    in_win = bool(w_lo <= pa[0] <= w_hi and w_lo <= pb[0] <= w_hi)
+    echo_rel = float(np.linalg.norm(a[k_lo:k_hi] - b[k_lo:k_hi]) / max(np.linalg.norm(b[k_lo:k_hi]), 1e-300))
+    return {"steps": nt, "trace_rel_l2": rel, "echo_window_s": [w_lo, w_hi], "pick_search_from_s": t_lo,
+            "echo_pick_s_f32_f64": [pa[0], pb[0]], "echo_pick_identical": same,
+            "echo_pick_in_window": in_win, "echo_rel_l2_after_burst": echo_rel,
+            "echo_to_burst_envelope": float(pb[1] / max(np.abs(b).max(), 1e-300))}
 
 
 def _e2e(p, steps, warm=True):
@@ -429,7 +454,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        p = _problem(args.workload, nt=max(K, W, 8))
+        # inputs built on the host only (the labeller's NumPy twin is
+        # bit-identical to the device labeller), so that this process loads
+        # no library of the CUDA path
+        p = _problem(args.workload, nt=max(K, W, 8), use_gpu=False)
         val, n, cores, kind, sample = _cpu_run(p, budget_s=90.0, max_steps=K, warmup=W)
         line = {"metric": "Gcell-updates/s", "value": val, "unit": "Gcell-updates/s",
                 "n_gpus": args.gpus, "steps": n, "warmup": W,
@@ -439,7 +467,7 @@ def main():
                 "config": {"workload": args.workload, "grid": list(p["lab"].shape),
                            "grains": int(p["n_grains"]), "timesteps_per_step": 1},
                 "cpu_baseline": {"value": val, "unit": "Gcell-updates/s", "cores": cores,
-                                 "kind": kind, "sample": sample},
+                                 "cpu_model": _cpu_model(), "kind": kind, "sample": sample},
                 "e2e": {"value": val, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -466,9 +494,10 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    p = _problem(args.workload, nt=W + K + 64)
+    n_total = max(W + K, SPLIT_FROM) + 64
+    p = _problem(args.workload, nt=n_total)
     ncell = int(np.prod(p["lab"].shape))
-    solve = _device_solve(p, W + K + 64)
+    solve = _device_solve(p, n_total)
 
     solve.run(0, W)
     torch.cuda.synchronize()
@@ -492,10 +521,15 @@ def main():
     tr = solve.traces_numpy(W + K)
     finite = bool(np.isfinite(tr).all())
 
-    # per-kernel split for the roofline (events around each launch), taken
-    # from the state the timed steps left (a filled wavefield: the first steps
-    # after a reset skip most face-density divisions and run faster)
-    ms_s, ms_v = solve.profile(min(50, K))
+    # per-kernel split for the roofline (events around each launch), taken on
+    # a filled wavefield: the first steps after a reset skip most face-density
+    # divisions and run faster, so the state is first advanced (untimed) to
+    # step SPLIT_FROM when the timed steps ended earlier
+    n_done = W + K
+    if n_done < SPLIT_FROM:
+        solve.run(n_done, SPLIT_FROM)
+        n_done = SPLIT_FROM
+    ms_s, ms_v = solve.profile(50)
     solve.close()
     peak, peak_kind = _peaks()
     step_ms = ms / K
@@ -525,19 +559,20 @@ def main():
                               "peak": peak, "unit": "GB/s",
                               "frac": ALG_BYTES_STEP * ncell / (step_ms / 1e3) / 1e9 / peak,
                               "alg_bytes_per_cell": ALG_BYTES_STEP,
-                              "kernel_ms": {"k_stress": ms_s, "k_velocity": ms_v}},
+                              "kernel_ms": {"k_stress": ms_s, "k_velocity": ms_v},
+                              "split_taken_after_steps": n_done, "split_steps": 50},
             "gpu_launches": launches, "traces_finite": finite}
     if rank == 0 and not args.no_e2e:
         line["e2e"] = _e2e(p, K)
     if rank == 0 and not args.no_cpu:
-        line["fp64_check"] = _fp64_check(p, W + K, tr)
+        line["fp64_check"] = _fp64_check(p, int(p["spec"]["nt"]))
     clk_sum = clk.summary()
     if clk_sum is not None:
         line["clocks"] = clk_sum
     if rank == 0 and not args.no_cpu and world == 1:
         val, n, cores, kind, sample = _cpu_run(p, budget_s=20.0, max_steps=200)
         line["cpu_baseline"] = {"value": val, "unit": "Gcell-updates/s", "cores": cores,
-                                "kind": kind, "sample": sample}
+                                "cpu_model": _cpu_model(), "kind": kind, "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

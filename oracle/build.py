@@ -21,7 +21,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE_ROOT = os.environ.get("PE_REFERENCE_ROOT", "/root/reference")
+
+
+def _reference_root():
+    """The reference checkout to read the kernel strings from
+    (PE_REFERENCE_ROOT): required to build oracle/_ref, no default; without
+    it the prebuilt library is used."""
+    return os.environ.get("PE_REFERENCE_ROOT")
+
 
 ORACLE_LIB = os.path.join(BUILD, "liboracle.so")
 REF_CPU_LIB = os.path.join(REF_OUT, "libref_cpu.so")
@@ -75,10 +82,18 @@ def _reference_kernel_sources(root):
 
 def build_ref(force=False):
     """Build oracle/_ref/libref_cpu.so; returns its path or None if impossible."""
-    core = os.path.join(REFERENCE_ROOT, "sim", "core", "fdtd.py")
     harness = os.path.join(HERE, "ref_harness.cpp")
+    REFERENCE_ROOT = _reference_root()
+    if not REFERENCE_ROOT:
+        if not os.path.exists(REF_CPU_LIB):
+            print("oracle/build.py: PE_REFERENCE_ROOT is not set, so oracle/_ref (the reference's "
+                  "own kernels built for the host) cannot be built; set it to the reference "
+                  "checkout to build it", file=sys.stderr)
+            return None
+        return REF_CPU_LIB
+    core = os.path.join(REFERENCE_ROOT, "sim", "core", "fdtd.py")
     if not os.path.exists(core):
-        return REF_CPU_LIB if os.path.exists(REF_CPU_LIB) else None
+        raise FileNotFoundError(f"PE_REFERENCE_ROOT={REFERENCE_ROOT!r} holds no sim/core/fdtd.py")
     if not force and _newer(REF_CPU_LIB, [core, harness, __file__]):
         return REF_CPU_LIB
     os.makedirs(REF_OUT, exist_ok=True)

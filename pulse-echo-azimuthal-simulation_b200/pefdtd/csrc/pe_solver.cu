@@ -887,7 +887,12 @@ int pe_solver_adjoint_segment(PeSolver *S, const PeState *state, const PeAdjoint
         for (int c = 0; c < 3; ++c) adj.v_prev[c] = hist + ((size_t)(n - a) * 3 + c) * fb;
         rc = S->cfg.dtype == PE_F64 ? adjoint_step_t<double>(S, &adj, n, residual, st, S->grad_rep, S->nrep)
                                     : adjoint_step_t<float>(S, &adj, n, residual, st, S->grad_rep, S->nrep);
-        if (rc) return rc;
+        if (rc) {
+            // the replicas hold partial sums of this segment: clear them, so
+            // that a later segment's fold starts from zero as it assumes
+            cudaMemsetAsync(S->grad_rep, 0, sizeof(double) * (size_t)(glen * S->nrep), st);
+            return rc;
+        }
     }
     pe::k_grad_fold<<<(unsigned)((glen + 255) / 256), 256, 0, st>>>(S->grad_rep, S->nrep, glen, adj0->grad);
     PE_CUDA(cudaGetLastError());

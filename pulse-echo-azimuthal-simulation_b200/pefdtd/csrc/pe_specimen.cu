@@ -7,6 +7,7 @@
 // (R2 is the caller's R**2, so the inside test matches bit for bit).
 // Compiled with -fmad=false so no product is fused into a sum, as in NumPy.
 // One thread per cell; seeds are staged through shared memory in tiles.
+#include <atomic>
 #include <cstdint>
 #include <string>
 
@@ -178,14 +179,19 @@ extern "C" int pe_label_cylinder(const double *xs, int nx, const double *ys, int
 // ------------------------------------------------------------------------------
 namespace {
 
-constexpr int NOALLOC_MAX_COORDS = 12288;
-constexpr int NOALLOC_MAX_SEEDS = 16384;
+constexpr int NOALLOC_MAX_COORDS = PE_NOALLOC_MAX_COORDS;
+constexpr int NOALLOC_MAX_SEEDS = PE_NOALLOC_MAX_SEEDS;
 constexpr size_t NOALLOC_DOUBLES = (size_t)NOALLOC_MAX_COORDS + 4 * (size_t)NOALLOC_MAX_SEEDS;
 
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+static_assert(sizeof(g_noalloc_scratch) == PE_NOALLOC_SCRATCH_BYTES,
+              "the array must be exactly the size the header documents");
 
+// per-device address of the array, looked up once; atomic, so that first
+// calls from several host threads do not race on the cache (they may each
+// look it up, and all store the same address)
 constexpr int NOALLOC_MAX_DEVICES = 64;
-double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+std::atomic<double *> g_noalloc_ptr[NOALLOC_MAX_DEVICES];
 
 thread_local std::string g_noalloc_err;
 
@@ -215,14 +221,13 @@ extern "C" int pe_label_cylinder_noalloc(const double *xs, int nx, const double 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
         return noalloc_fail(PE_ERR_CUDA, "no usable current device");
-    if (!g_noalloc_ptr[dev]) {
-        double *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
+    double *d = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!d) {
+        const cudaError_t e = cudaGetSymbolAddress((void **)&d, g_noalloc_scratch);
+        if (e != cudaSuccess || !d)
             return noalloc_fail(PE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = p;
+        g_noalloc_ptr[dev].store(d, std::memory_order_release);
     }
-    double *d = g_noalloc_ptr[dev];
     cudaStream_t st = (cudaStream_t)stream;
     double *dx = d, *dy = dx + nx, *dz = dy + ny, *ds = d + NOALLOC_MAX_COORDS, *dw = ds + 3 * (size_t)ns;
     cudaError_t e = cudaMemcpyAsync(dx, xs, sizeof(double) * nx, cudaMemcpyHostToDevice, st);

@@ -315,10 +315,12 @@ cudaError_t stage(Staged &s, cudaStream_t st, std::initializer_list<std::pair<co
     size_t total = 0;
     for (auto &q : parts) total += (q.second + 255) & ~size_t(255);
     if (total > a.cap) {
+        // grow geometrically, so that a run of ever larger calls reallocates
+        // (and synchronises the device in cudaFree) only O(log) times
+        const size_t want = std::max(total, std::max(a.cap * 2, (size_t)1 << 16));
         if (a.p) cudaFree(a.p);
         a.p = nullptr;
         a.cap = 0;
-        const size_t want = std::max(total, std::max(a.cap * 2, (size_t)1 << 16));
         e = cudaMalloc(&a.p, want);
         if (e != cudaSuccess) {
             a.p = nullptr;

@@ -20,6 +20,8 @@ reference builds (x, y, z) and transposes, which is the same map.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from .materials import rotation_z_to
@@ -38,7 +40,7 @@ def seed_points(R, thickness, n, rng):
     return s
 
 
-def label_cylinder_numpy(xs, ys, zs, R, seeds, weights=None, chunk=1 << 16):
+def label_cylinder_numpy(xs, ys, zs, R, seeds, weights=None, chunk=1 << 13):
     """(nz, ny, nx) int32 power-diagram labels; -1 outside the cylinder."""
     xs, ys, zs = (np.asarray(a, float) for a in (xs, ys, zs))
     seeds = np.asarray(seeds, float)
@@ -47,15 +49,26 @@ def label_cylinder_numpy(xs, ys, zs, R, seeds, weights=None, chunk=1 << 16):
     inside = (X ** 2 + Y ** 2) <= R ** 2
     P = np.stack([X[inside], Y[inside]], axis=1)
     out = np.full((len(zs), len(ys), len(xs)), -1, np.int32)
-    lab_plane = np.empty(len(P), np.int32)
-    for iz, z in enumerate(zs):
-        dz2 = (z - seeds[:, 2]) ** 2
+
+    def plane(iz):
+        # each plane is independent: the same element-wise arithmetic whichever
+        # thread runs it (NumPy releases the GIL inside the array operations)
+        dz2 = (zs[iz] - seeds[:, 2]) ** 2
+        lab_plane = np.empty(len(P), np.int32)
         for a in range(0, len(P), chunk):
             p = P[a:a + chunk]
             d = (((p[:, None, :] - seeds[None, :, :2]) ** 2).sum(-1) - w[None, :]) + dz2[None, :]
             lab_plane[a:a + chunk] = d.argmin(axis=1)
-        plane = out[iz]
-        plane[inside] = lab_plane
+        out[iz][inside] = lab_plane
+
+    n_threads = max(1, min(len(zs), os.cpu_count() or 1))
+    if n_threads == 1:
+        for iz in range(len(zs)):
+            plane(iz)
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(n_threads) as ex:
+            list(ex.map(plane, range(len(zs))))
     return out
 
 

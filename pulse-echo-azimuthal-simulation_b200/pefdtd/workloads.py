@@ -112,3 +112,25 @@ def make_problem(name_or_spec, nt=None, use_gpu=None, kh_max=2.0):
                 nt=nt, coeffs=coeffs, wavelet=wav, src_pts=[(p, w) for p in pts],
                 rec_groups=[(pts, np.full(len(pts), w))], sponge=spec["sponge"],
                 record="vz")
+
+
+def bottom_echo_window(p):
+    """Where the disk's bottom-face echo must be picked, for a problem from
+    make_problem: (t_lo, win_lo, win_hi) in seconds.
+
+    The probe sits on the top ice face, so the echo travels 2 x height through
+    ice. Vertical qP speeds of the hexagonal ice lie between sqrt(C11 / rho)
+    (c-axis horizontal) and sqrt(C33 / rho) (c-axis vertical); the window
+    spans those round trips with a 5 % margin, plus the burst length for the
+    echo's envelope. t_lo, the start of the pick's search, lies halfway
+    between the end of the transmitted burst and the earliest echo, so the
+    transmitted burst is outside the search."""
+    from .materials import ICE
+    spec = p["spec"]
+    H = float(spec["height"])
+    c_fast = np.sqrt(ICE["C33"] / ICE["rho"])
+    c_slow = np.sqrt(ICE["C11"] / ICE["rho"])
+    burst = spec["n_cycles"] / spec["f0"]
+    win_lo = 2.0 * H / (1.05 * c_fast)
+    win_hi = 2.0 * H / (0.95 * c_slow) + burst
+    return 0.5 * (burst + win_lo), win_lo, win_hi

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ by importing the reference.
 
-Run where the reference tree is present (default /root/reference, override
-with PE_REFERENCE_ROOT):  python tests/golden/make_golden.py
+Run where the reference tree is present, with PE_REFERENCE_ROOT naming it:
+  PE_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 
 Every fixture records what the reference itself computes for seeded inputs
 (the inputs are stored beside the outputs, so the tests need no reference at
@@ -28,7 +28,10 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("PE_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("PE_REFERENCE_ROOT")
+if not REF or not os.path.isdir(os.path.join(REF, "sim", "core")):
+    raise SystemExit("make_golden.py imports the reference: set PE_REFERENCE_ROOT to its checkout "
+                     "(the directory holding sim/core/fdtd.py)")
 sys.path[:0] = [os.path.join(REF, "sim", "core"), os.path.join(REF, "vendor"),
                 os.path.join(REF, "sim", "fw_checks")]
 

@@ -55,6 +55,32 @@ def test_noalloc_matches_allocating_entry_twice():
         assert int((ref >= 0).sum()) > 0
 
 
+def test_noalloc_at_the_exact_limits():
+    """nx + ny + nz and the seed count at their maxima: the coordinate and the
+    seed / weight slices then reach the last element of the array."""
+    import torch
+    from pefdtd import specimen
+    L, capi = _lib()
+    rng = np.random.default_rng(23)
+    nx = 12288 - 2
+    xs = np.ascontiguousarray((np.arange(nx) - (nx - 1) / 2) * 1e-6)
+    ys = np.zeros(1)
+    zs = np.zeros(1)
+    R = 4e-3
+    seeds = np.ascontiguousarray(specimen.seed_points(R, 2e-3, 16384, rng))
+    w = np.ascontiguousarray(rng.uniform(0, 3e-7, len(seeds)))
+    for weights in (w, None):
+        ref = torch.full((1, 1, nx), -7, dtype=torch.int32, device="cuda")
+        got = torch.full_like(ref, -9)
+        capi.check(_call(L.pe_label_cylinder, capi, xs, ys, zs, R, seeds, weights, ref))
+        for _ in range(2):
+            got.fill_(-9)
+            rc = _call(L.pe_label_cylinder_noalloc, capi, xs, ys, zs, R, seeds, weights, got)
+            assert rc == 0, L.pe_label_cylinder_noalloc_error().decode()
+            assert torch.equal(got, ref)
+        assert int((ref >= 0).sum()) > 0
+
+
 def test_noalloc_refuses_oversized_requests():
     import torch
     L, capi = _lib()
