@@ -49,6 +49,7 @@ ALG_BYTES_STEP = 74      # 9 f32 fields read + written, u16 label read, per cell
 ALG_BYTES_STRESS = 62    # v read 12, s read 24 + write 24, label 2
 ALG_BYTES_VEL = 50       # s read 24, v read 12 + write 12, label 2
 SPLIT_FROM = 300         # the per-kernel split is taken from this step on (filled wavefield)
+SWEEP_STEPS = 200        # steps per solve of the compact 36-azimuth sweep in the default line
 
 
 def _peaks():
@@ -343,6 +344,121 @@ def _sweep(args):
                        "timing": "wall clock, set-up and trace download included, synchronised"}}
 
 
+def _azimuth_host(base, az):
+    """The reference's per-azimuth set-up on the host (sweep_runner.py:322-390):
+    the label volume and the c-axes turned by -az (NumPy resample), the
+    material tables, the probe on the rotated grid."""
+    from pefdtd import inversion, materials, workloads
+    lab = inversion.rotate_labels(base["lab"], az)
+    a = np.radians(az)
+    R = np.array([[np.cos(a), -np.sin(a), 0.0], [np.sin(a), np.cos(a), 0.0], [0.0, 0.0, 1.0]])
+    axes = np.asarray(base["axes"], float) @ R
+    Ct, rho = materials.material_tables(axes)
+    pts = workloads.top_probe(lab, base["h"], base["spec"]["aperture"])
+    w = 1.0 / len(pts)
+    return dict(base, lab=lab, mats=(lab + 1).astype(np.uint16), axes=axes, Ct=Ct, rho_t=rho,
+                src_pts=[(q, w) for q in pts], rec_groups=[(pts, np.full(len(pts), w))])
+
+
+def _azimuth_specs_device(base, azs):
+    """The batched set-up: one upload of the label volume, every azimuth's
+    rotated labels gathered on the device (the same nearest-cell resample),
+    tables and probe (one plane) on the host."""
+    import torch
+    from pefdtd import batch, inversion, materials, workloads
+    nz, ny, nx = base["lab"].shape
+    lab_d = torch.from_numpy(np.ascontiguousarray(base["lab"], np.int32)).cuda()
+    iz = int(np.nonzero((base["lab"] >= 0).any(axis=(1, 2)))[0][0])
+    X, Y = np.meshgrid(np.arange(nx) - (nx - 1) / 2.0, np.arange(ny) - (ny - 1) / 2.0, indexing="xy")
+    specs = []
+    for az in azs:
+        a = np.radians(az)
+        ca, sa = np.cos(a), np.sin(a)
+        xs = np.rint(ca * X - sa * Y + (nx - 1) / 2.0).astype(np.int64)
+        ys = np.rint(sa * X + ca * Y + (ny - 1) / 2.0).astype(np.int64)
+        ok = (xs >= 0) & (xs < nx) & (ys >= 0) & (ys < ny)
+        flat = torch.from_numpy(np.where(ok, np.clip(ys, 0, ny - 1) * nx + np.clip(xs, 0, nx - 1), -1)).cuda()
+        src = lab_d.reshape(nz, ny * nx)[:, flat.clamp(min=0).reshape(-1)].reshape(nz, ny, nx)
+        mats = torch.where(flat.reshape(1, ny, nx) >= 0, src + 1, torch.zeros_like(src))
+        plane = inversion.rotate_labels(base["lab"][iz:iz + 1], az)
+        full = np.full((iz + 1, ny, nx), -1, np.int32)
+        full[iz] = plane[0]
+        pts = workloads.top_probe(full, base["h"], base["spec"]["aperture"])
+        w = 1.0 / len(pts)
+        R = np.array([[ca, -sa, 0.0], [sa, ca, 0.0], [0.0, 0.0, 1.0]])
+        Ct, rho = materials.material_tables(np.asarray(base["axes"], float) @ R)
+        p = dict(base, Ct=Ct, rho_t=rho, src_pts=[(q, w) for q in pts],
+                 rec_groups=[(pts, np.full(len(pts), w))])
+        sp = batch.spec_from_problem(p)
+        sp["mats"] = mats
+        specs.append(sp)
+    return specs
+
+
+def _sweep_compact(K, workload="disk_small", n_az=36):
+    """A 36-azimuth sweep of one disk and its misfit gradients, each run as
+    the reference runs it (one azimuth at a time: host set-up, upload, solve,
+    read back) and batched (device-side set-up, one batch). Wall clock,
+    synchronised; traces and gradients compared between the arms."""
+    import torch
+    from pefdtd import adjoint, batch, inversion, workloads
+    base = workloads.make_problem(workload, nt=K)
+    azs = [360.0 * i / n_az for i in range(n_az)]
+    cells = int(np.prod(base["lab"].shape))
+    # warm-up of both paths (library, allocator, graph capture)
+    sv = _device_solve(_azimuth_host(base, 0.0), K)
+    sv.run(0, 8)
+    sv.close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = []
+    for az in azs:
+        sv = _device_solve(_azimuth_host(base, az), K)
+        sv.run(0, K)
+        plain.append(sv.traces_numpy(K))
+        sv.close()
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b = batch.BatchSolver(_azimuth_specs_device(base, azs))
+    try:
+        b.run(0, K)
+        got = b.traces_numpy(K)
+    finally:
+        b.close()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    same = all(np.array_equal(a, g[:K]) for a, g in zip(plain, got))
+    out = {"azimuths": n_az, "steps": K, "workload": workload, "cells_per_solve": cells,
+           "plain_s": t_plain, "batched_s": t_batch, "speedup": t_plain / t_batch,
+           "traces_identical": bool(same),
+           "plain": "per azimuth: host rotation of labels and axes, tables, probe, upload, solve, read back",
+           "batched": "labels uploaded once and rotated on the device, one batch of all azimuths"}
+    # the gradients of the same sweep (misfit against the traces of a
+    # perturbed fabric), one at a time and batched
+    disk = inversion.Disk(workload, azs, nt=K, dtype="float32", checkpoint_every=200)
+    th, ph = adjoint.angles_from_axes(disk.true_axes)
+    th_t, ph_t = torch.as_tensor(th), torch.as_tensor(ph)
+    c21s = [inversion.tables21(th_t, ph_t, az).numpy() for az in azs]
+    dobs = [g[:K] * 1.01 for g in got]
+    adjoint.misfit_gradients(disk.problems[:1], c21s[:1], dobs[:1])   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    one = [adjoint.misfit_gradients([p], [c], [d])[0] for p, c, d in zip(disk.problems, c21s, dobs)]
+    torch.cuda.synchronize()
+    tg_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    many = adjoint.misfit_gradients(disk.problems, c21s, dobs)
+    torch.cuda.synchronize()
+    tg_batch = time.perf_counter() - t0
+    dev = max(float(np.abs(g - q).max() / max(np.abs(q).max(), 1e-300)) for (_, g), (_, q) in zip(many, one))
+    out["gradients"] = {"solves": n_az, "steps": K, "plain_s": tg_plain, "batched_s": tg_batch,
+                        "speedup": tg_plain / tg_batch, "max_rel_grad_diff": dev,
+                        "checkpoint_every": 200}
+    out["sweep_plus_gradients_speedup"] = (t_plain + tg_plain) / (t_batch + tg_batch)
+    return out
+
+
 def _traces(args):
     """Device vs host post-processing of N records of the workload's length
     (sweep analysis and high-passed picks; one line of JSON)."""
@@ -389,47 +505,117 @@ def _traces(args):
 
 
 def _gradients(args):
-    """Misfits and stiffness gradients of N solves: one at a time vs
-    pefdtd.adjoint.misfit_gradients (one line of JSON)."""
+    """Misfit gradients of an N-azimuth sweep of one disk (the gradient
+    configuration: checkpoints every 200 steps, recomputation, the memory
+    plan of pefdtd.adjoint deciding waves, two-level checkpoints and host
+    offload for the free HBM): one at a time vs batched (one line of JSON)."""
     import torch
-    from pefdtd import workloads
-    from pefdtd.adjoint import Problem, misfit_gradients
-    from pefdtd.fdtd import _material_tables64
-    from pefdtd.materials import c36_to_c21
+    from pefdtd import adjoint, inversion
     K = int(args.steps)
-    probs, c21s, dobs, cells = [], [], [], 0
-    for i in range(int(args.gradients)):
-        spec = dict(workloads.WORKLOADS[args.workload], seed=11 + i)
-        p = workloads.make_problem(spec, nt=K)
-        probs.append(Problem(p["mats"], p["rho_t"], p["h"], p["dt"], p["coeffs"], p["src_pts"],
-                             p["rec_groups"], p["wavelet"], record="vz", sponge_width=p["sponge"],
-                             dtype="float32", checkpoint_every=200))
-        c21s.append(c36_to_c21(_material_tables64(p["axes"], 1500.0, 300.0)[0]))
-        dobs.append(np.zeros((K, 1)))
-        cells += int(np.prod(p["lab"].shape))
-    misfit_gradients(probs[:1], c21s[:1], dobs[:1])   # warm-up (library, allocator)
+    n = int(args.gradients)
+    azs = [360.0 * i / n for i in range(n)]
+    disk = inversion.Disk(args.workload, azs, nt=K, dtype="float32", checkpoint_every=200)
+    th, ph = adjoint.angles_from_axes(disk.true_axes)
+    th_t, ph_t = torch.as_tensor(th), torch.as_tensor(ph)
+    c21s = [inversion.tables21(th_t, ph_t, az).numpy() for az in azs]
+    # observed data: the traces of the same disk with its c-axes re-drawn
+    rng = np.random.default_rng(int(disk.base["spec"]["seed"]) + 1)
+    th2, ph2 = inversion.isotropic_angles(disk.n_grains, rng)
+    dobs = [pr.traces_numpy(inversion.tables21(torch.as_tensor(th2), torch.as_tensor(ph2), az).numpy())
+            for pr, az in zip(disk.problems[:1], azs[:1])] * n
+    free = torch.cuda.mem_get_info()[0]
+    budget = int(0.8 * free)
+    waves = adjoint.plan_waves(disk.problems, budget)
+    adjoint.misfit_gradients(disk.problems[:1], c21s[:1], dobs[:1])   # warm-up
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    plain = []
-    for pr, c, d in zip(probs, c21s, dobs):
-        a = pr.make_adjoint(c)
-        tr = a.forward().to(torch.float64)
-        r = tr - torch.as_tensor(d, device=tr.device)
-        plain.append(a.backward(r))
-        a.solve.close()
-    torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    got = misfit_gradients(probs, c21s, dobs)
+    many = adjoint.misfit_gradients(disk.problems, c21s, dobs, memory_budget=budget)
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
-    dev = max(float(np.abs(g - q).max() / max(np.abs(q).max(), 1e-300)) for (_, g), q in zip(got, plain))
+    peak = torch.cuda.max_memory_allocated()
+    n_plain = min(n, int(args.plain_solves) if args.plain_solves else n)
+    t0 = time.perf_counter()
+    one = [adjoint.misfit_gradients([p], [c], [d], memory_budget=budget)[0]
+           for p, c, d in zip(disk.problems[:n_plain], c21s[:n_plain], dobs[:n_plain])]
+    torch.cuda.synchronize()
+    t_plain = (time.perf_counter() - t0) * n / n_plain
+    dev = max(float(np.abs(g - q).max() / max(np.abs(q).max(), 1e-300)) for (_, g), (_, q) in zip(many, one))
+    shape = disk.base["lab"].shape
+    plan = sorted({opt for w in waves for _, opt in w})
     return {"metric": "misfit + gradient solves/s, batched vs plain loop", "unit": "solves/s",
-            "solves": len(probs), "steps": K, "cells_per_solve": cells // len(probs),
-            "plain": len(probs) / t_plain, "batched": len(probs) / t_batch, "speedup": t_plain / t_batch,
-            "plain_s": t_plain, "batched_s": t_batch, "max_rel_grad_diff": dev,
+            "solves": n, "steps": K, "grid": list(shape), "grains": disk.n_grains,
+            "angles": 2 * disk.n_grains, "plain": n / t_plain, "batched": n / t_batch,
+            "speedup": t_plain / t_batch, "plain_s": t_plain, "batched_s": t_batch,
+            "plain_solves_timed": n_plain, "max_rel_grad_diff": dev,
+            "waves": [len(w) for w in waves], "plan_inner_offload": [list(o) for o in plan],
+            "bytes_per_solve_unplanned": adjoint.adjoint_bytes(shape, K, 200),
+            "device_budget_bytes": budget, "peak_allocated_bytes": int(peak),
             "config": {"workload": args.workload, "dtype": "f32", "checkpoint_every": 200,
                        "timing": "wall clock; solver creation, forward, adjoint and gradient download included"}}
+
+
+def _inversion_specs(n):
+    """Disks of mixed sizes and fabrics for the inversion (seeded): grids from
+    64 x 96 x 96 to 80 x 128 x 128 at h = 0.2 mm, 40-120 grains,
+    single-maximum (Watson kappa 5-20 about an axis 30 deg from z) and girdle
+    fabrics, 1 MHz 3-cycle burst, 8-cell sponge (both disk faces outside it,
+    so the bottom echo reaches the probe)."""
+    out = []
+    for i in range(n):
+        f = i / max(1, n - 1)
+        nxy = int(round((96 + 32 * f) / 16)) * 16
+        nz = int(round((64 + 16 * f) / 8)) * 8
+        h = 0.2e-3
+        fabric = ("watson", 30.0, 5.0 + 15.0 * f) if i % 2 == 0 else ("girdle", 20.0, 10.0)
+        out.append(dict(shape=(nz, nxy, nxy), h=h, diameter=(nxy - 22) * h, height=(nz - 22) * h,
+                        n_grains=int(40 + 80 * ((3 * i) % n) / max(1, n - 1)), fabric=fabric,
+                        f0=1.0e6, n_cycles=3, nt=2000, sponge=8, aperture=6e-3, seed=300 + i))
+    return out
+
+
+def _inversion(args):
+    """The batched gradient fabric inversion (pefdtd.inversion): D disks x A
+    azimuths, L-BFGS on every grain's (theta, phi) from an isotropic fabric,
+    batched; the plain loop's evaluation timed once beside it (one line)."""
+    import torch
+    from pefdtd import inversion
+    D, A, K, I = int(args.inversion), int(args.azimuths), int(args.steps), int(args.iterations)
+    azs = [360.0 * i / A for i in range(A)]
+    disks = [inversion.Disk(sp, azs, nt=K, dtype="float32", checkpoint_every=200)
+             for sp in _inversion_specs(D)]
+    d_obs = inversion.observe(disks)
+    rng = np.random.default_rng(11)
+    x0 = np.concatenate([a for d in disks for a in inversion.isotropic_angles(d.n_grains, rng)])
+    inv = inversion.FabricInversion(disks, d_obs, batched=True)
+    plain = inversion.FabricInversion(disks, d_obs, batched=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Jp, gp = plain.objective(x0)
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Jb, gb = inv.objective(x0)
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res = inv.run(x0, iterations=I)
+    t_run = time.perf_counter() - t0
+    errs0, errs = [], []
+    for d, (th, ph), (th0, ph0) in zip(disks, inv.split(res["x"]), inv.split(x0)):
+        errs.append(inversion.eigen_error(inversion.axes_of(th, ph), d.true_axes))
+        errs0.append(inversion.eigen_error(inversion.axes_of(th0, ph0), d.true_axes))
+    return {"metric": "L-BFGS fabric inversion, wall time per iteration", "unit": "s/iteration",
+            "disks": D, "azimuths": A, "solves_per_evaluation": D * A, "steps": K,
+            "grids": [list(d.base["lab"].shape) for d in disks], "grains": [d.n_grains for d in disks],
+            "parameters": int(len(x0)), "iterations": res["iterations"], "evaluations": res["evaluations"],
+            "s_per_iteration": t_run / max(1, res["iterations"]),
+            "per_iteration": res["per_iteration"], "J0": res["J0"], "J": res["J"],
+            "evaluation_s_batched": t_batch, "evaluation_s_plain": t_plain,
+            "evaluation_speedup": t_plain / t_batch,
+            "plain_equals_batched": {"J_rel": abs(Jb - Jp) / abs(Jp),
+                                     "grad_rel": float(np.abs(gb - gp).max() / np.abs(gp).max())},
+            "eigenvalue_error_start": errs0, "eigenvalue_error_end": errs,
+            "config": {"dtype": "f32", "checkpoint_every": 200, "start": "isotropic (seeded)",
+                       "observed": "synthetic traces of the true fabric, same solver",
+                       "timing": "wall clock per iteration: all batched forward+adjoint evaluations of the line search"}}
 
 
 def main():
@@ -441,10 +627,15 @@ def main():
     ap.add_argument("--workload", default="disk_prod")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--sweep", type=int, default=0)
     ap.add_argument("--uneven", action="store_true")
     ap.add_argument("--traces", type=int, default=0)
     ap.add_argument("--gradients", type=int, default=0)
+    ap.add_argument("--plain-solves", type=int, default=0)
+    ap.add_argument("--inversion", type=int, default=0)
+    ap.add_argument("--azimuths", type=int, default=36)
+    ap.add_argument("--iterations", type=int, default=10)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -484,6 +675,10 @@ def main():
     if args.gradients:
         if rank == 0:
             print(json.dumps(_gradients(args)), flush=True)
+        return
+    if args.inversion:
+        if rank == 0:
+            print(json.dumps(_inversion(args)), flush=True)
         return
 
     import torch
@@ -566,6 +761,8 @@ def main():
         line["e2e"] = _e2e(p, K)
     if rank == 0 and not args.no_cpu:
         line["fp64_check"] = _fp64_check(p, int(p["spec"]["nt"]))
+    if rank == 0 and not args.no_sweep:
+        line["sweep"] = _sweep_compact(SWEEP_STEPS)
     clk_sum = clk.summary()
     if clk_sum is not None:
         line["clocks"] = clk_sum

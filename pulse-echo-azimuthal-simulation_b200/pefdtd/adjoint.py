@@ -6,18 +6,25 @@ cell-density adjoint that stores the whole velocity history
 vendor/ringfwi/axisfield.py:37-161. Here:
 
 * :class:`AdjointSolve` runs the production forward scheme on the GPU,
-  keeping full-state checkpoints every ``checkpoint_every`` steps in device
-  memory; the reverse sweep recomputes each segment from its checkpoint,
-  keeping that segment's velocity history, and applies the exact discrete
+  keeping full-state checkpoints every ``checkpoint_every`` steps (in device
+  memory, or in pinned host memory with ``offload=True``); the reverse sweep
+  recomputes each segment from its checkpoint and applies the exact discrete
   adjoint step (csrc/pe_adjoint.cuh) backwards through it, accumulating
-  dJ/dC for every material's 21 stiffness constants.
+  dJ/dC for every material's 21 stiffness constants. With ``inner_every=m``
+  the checkpointing is two-level: a segment is first recomputed keeping
+  full-state checkpoints every m steps, and only m steps of velocity history
+  are held at a time (memory ~ (K/m) states + m velocity fields instead of
+  K velocity fields; ``plan_memory`` picks K, m and the offload for a byte
+  budget). The reference keeps the whole velocity history
+  (vendor/ringfwi/elastic3d.py:301,305).
 * :class:`StiffnessTraces` is a ``torch.autograd.Function`` from the
   per-material table ``(n_mat, 21)`` to the traces ``(nt, n_groups)``; its
   backward is that adjoint with the incoming trace gradient as the adjoint
   source, so any loss on the traces (``0.5*||tr - d||^2`` gives the
   reference's misfit) differentiates through it.
 * :func:`misfit_gradients` runs the misfits and gradients of many solves
-  together, their segments interleaved on one CUDA stream per solve.
+  together, their segments interleaved on one CUDA stream per solve, in
+  waves whose device memory fits the free HBM.
 * :func:`ice_table21` builds that table differentiably from per-grain c-axis
   angles (colatitude theta, azimuth phi; R = Rz(phi) Ry(theta), the
   convention of vendor/ringfwi/axisfield.py:37-65 and cof.axes_from_params),
@@ -51,17 +58,60 @@ def _bind():
     return L
 
 
+def adjoint_bytes(shape, nt, checkpoint_every=200, inner_every=None, offload=False, esize=4,
+                  damp_volume=False):
+    """Device bytes of one misfit-and-gradient solve (AdjointSolve): the
+    solver (state, labels, damping volume), the outer checkpoints (none on
+    the device when offloaded), the inner checkpoints and velocity history of
+    one reverse segment, and the adjoint state with its 33-field scratch."""
+    ncell = int(np.prod(shape))
+    field = ncell * esize
+    K = max(1, int(checkpoint_every))
+    m = min(K, int(inner_every)) if inner_every else K
+    solve = 9 * field + 2 * ncell + (4 * ncell if damp_volume else 0)
+    outer = 0 if offload else -(-int(nt) // K) * 9 * field
+    inner = (-(-min(K, int(nt)) // m)) * 9 * field if m < K else 0
+    hist = min(m, int(nt)) * 3 * field
+    adj = (9 + 33) * field
+    return solve + outer + inner + hist + adj
+
+
+def plan_memory(shape, nt, budget_bytes, checkpoint_every=200, esize=4, damp_volume=False):
+    """(inner_every, offload) for one solve under budget_bytes of device
+    memory, preferring no recomputation, then two-level checkpointing with
+    the inner spacing that minimises memory (m ~ sqrt(3 K): K/m states of 9
+    fields against m velocity fields of 3), then offloading the outer
+    checkpoints to pinned host memory. None if even that does not fit."""
+    K = max(1, int(checkpoint_every))
+    m_best = max(1, min(K, int(round(np.sqrt(3.0 * K)))))
+    for inner, off in ((None, False), (m_best, False), (None, True), (m_best, True)):
+        if adjoint_bytes(shape, nt, K, inner, off, esize, damp_volume) <= budget_bytes:
+            return inner, off
+    return None
+
+
 class AdjointSolve:
     """Forward with checkpoints, then reverse sweeps, on one DeviceSolve."""
 
-    def __init__(self, solve: DeviceSolve, checkpoint_every=200):
+    def __init__(self, solve: DeviceSolve, checkpoint_every=200, inner_every=None, offload=False):
         self.solve = solve
         self.K = int(checkpoint_every)
         if self.K < 1:
             raise ValueError("checkpoint_every must be >= 1")
+        self.m = self.K if not inner_every else min(self.K, int(inner_every))
+        if self.m < 1:
+            raise ValueError("inner_every must be >= 1")
+        self.offload = bool(offload)
         self.torch = solve.torch
         self.ckpt = {}
         self.nt = 0
+
+    def _save(self, state):
+        if self.offload:
+            h = self.torch.empty(state.shape, dtype=state.dtype, device="cpu", pin_memory=True)
+            h.copy_(state, non_blocking=True)   # stream-ordered before the next steps
+            return h
+        return state.clone()
 
     def forward(self, nt=None):
         """Traces (nt, n_groups) as a device tensor; keeps checkpoints."""
@@ -79,7 +129,7 @@ class AdjointSolve:
         self.ckpt = {}
         self.nt = nt
         for a in range(0, nt, self.K):
-            self.ckpt[a] = s.state.clone()
+            self.ckpt[a] = self._save(s.state)
             s.run(a, min(a + self.K, nt))
             yield a
 
@@ -111,7 +161,7 @@ class AdjointSolve:
             lam = torch.zeros((9,) + shape, dtype=tdt, device=dev)
             scratch = torch.zeros((33,) + shape, dtype=tdt, device=dev)
             grad = torch.zeros((s.cfg.n_mat, 21), dtype=torch.float64, device=dev)
-            hist = torch.empty((min(self.K, nt), 3) + shape, dtype=tdt, device=dev)
+            hist = torch.empty((min(self.m, nt), 3) + shape, dtype=tdt, device=dev)
         adj = _PeAdjoint()
         for i in range(3):
             adj.lv[i] = lam[i].data_ptr()
@@ -120,32 +170,101 @@ class AdjointSolve:
         adj.scratch = scratch.data_ptr()
         adj.grad = grad.data_ptr()
         stream = torch.cuda.current_stream(dev)
-        for a in reversed(sorted(self.ckpt)):
-            b = min(a + self.K, nt)
-            s.state.copy_(self.ckpt[a])
-            # recompute the segment and step back through it in one C call
+
+        def reverse(a, b):
+            # recompute [a, b) from the state and step back through it in one C call
             with torch.cuda.device(dev):
                 _capi.check(L.pe_solver_adjoint_segment(s._h, C.byref(s._st), C.byref(adj), hist.data_ptr(),
                                                         a, b, res.data_ptr(), C.c_void_p(stream.cuda_stream)))
+
+        for a in reversed(sorted(self.ckpt)):
+            b = min(a + self.K, nt)
+            s.state.copy_(self.ckpt[a], non_blocking=True)
+            if self.m >= b - a:
+                reverse(a, b)
+            else:
+                # two levels: inner checkpoints every m steps of the segment,
+                # then the sub-segments last first, m steps of history each
+                inner = {}
+                for a2 in range(a, b, self.m):
+                    inner[a2] = s.state.clone()
+                    s.run(a2, min(a2 + self.m, b))
+                for a2 in reversed(sorted(inner)):
+                    s.state.copy_(inner[a2])
+                    reverse(a2, min(a2 + self.m, b))
+                del inner
             yield grad
 
 
-def misfit_gradients(problems, c21s, dobs):
+def misfit_gradients(problems, c21s, dobs, memory_budget=None, plan=True):
     """J_i = 0.5 ||traces_i(c21_i) - dobs_i||^2 and dJ_i/dc21_i for many
     problems at once (a sweep's azimuths, an inversion's specimens): the
     checkpoint segments of every solve, forward then reverse, are issued
     round-robin on one CUDA stream per solve, so that solves too small to
     fill the GPU run side by side. Per solve the same kernels run in the same
     order as in the one-at-a-time gradient; only the order of the gradient's
-    atomic float64 sums may differ. Returns a list of (J, grad (n_mat_i, 21)
-    float64 numpy)."""
+    atomic float64 sums may differ.
+
+    The solves run in waves: each wave holds as many solves as fit
+    ``memory_budget`` bytes of device memory (default: 80 % of the free
+    memory when the call starts), each solve's checkpointing chosen by
+    plan_memory for its share when ``plan`` is set (two-level checkpoints,
+    host offload) so that even one large solve fits. Returns a list of
+    (J, grad (n_mat_i, 21) float64 numpy)."""
     torch = _torch()
     if not (len(problems) == len(c21s) == len(dobs)):
         raise ValueError("one table and one observed record per problem")
+    if not problems:
+        return []
+    if memory_budget is None:
+        dev = problems[0].device
+        with torch.cuda.device(dev if dev is not None else torch.cuda.current_device()):
+            memory_budget = int(0.8 * torch.cuda.mem_get_info()[0])
+    waves = plan_waves(problems, memory_budget, plan=plan)
+    out = [None] * len(problems)
+    for wave in waves:
+        res = _misfit_gradients_wave([problems[i] for i, _ in wave], [c21s[i] for i, _ in wave],
+                                     [dobs[i] for i, _ in wave], [opt for _, opt in wave])
+        for (i, _), r in zip(wave, res):
+            out[i] = r
+    return out
+
+
+def plan_waves(problems, budget, plan=True):
+    """Groups of (problem index, (inner_every, offload)) whose summed
+    adjoint_bytes fit the budget, in problem order."""
+    waves, cur, used = [], [], 0
+    for i, p in enumerate(problems):
+        shape = p.mats.shape
+        nt = len(p.wavelet)
+        es = 8 if p.dtype in ("float64", np.float64) else 4
+        dv = p.damp_mask is not None
+        opt = (p.inner_every, p.offload)
+        need = adjoint_bytes(shape, nt, p.K, opt[0], opt[1], es, dv)
+        if plan and need > budget:
+            got = plan_memory(shape, nt, budget, p.K, es, dv)
+            if got is None:
+                raise MemoryError(f"one gradient solve of {shape} x {nt} steps needs more than "
+                                  f"{budget / 2**30:.1f} GiB of device memory even with two-level "
+                                  "checkpoints and host offload")
+            opt = got
+            need = adjoint_bytes(shape, nt, p.K, opt[0], opt[1], es, dv)
+        if cur and used + need > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append((i, opt))
+        used += need
+    if cur:
+        waves.append(cur)
+    return waves
+
+
+def _misfit_gradients_wave(problems, c21s, dobs, opts):
+    torch = _torch()
     adjs = []
     try:
-        for p, c in zip(problems, c21s):
-            adjs.append(p.make_adjoint(np.asarray(c, float)))
+        for p, c, (inner, off) in zip(problems, c21s, opts):
+            adjs.append(p.make_adjoint(np.asarray(c, float), inner_every=inner, offload=off))
         streams = [torch.cuda.Stream(device=a.solve.device) for a in adjs]
         for st, a in zip(streams, adjs):
             st.wait_stream(torch.cuda.current_stream(a.solve.device))
@@ -223,7 +342,7 @@ class Problem:
 
     def __init__(self, mats, rho_t, h, dt, coeffs, src_pts, rec_groups, wavelet, record="vz",
                  sponge_width=0, damp_mask=None, damped_record=True, dtype="float64",
-                 checkpoint_every=200, device=None):
+                 checkpoint_every=200, device=None, inner_every=None, offload=False):
         from .damping import sponge_axis_profiles
         from .fdtd import _flat_probe
         self.mats = np.asarray(mats)
@@ -239,9 +358,11 @@ class Problem:
         self.damped_record = damped_record
         self.dtype = dtype
         self.K = checkpoint_every
+        self.inner_every = inner_every
+        self.offload = offload
         self.device = device
 
-    def make_adjoint(self, c21):
+    def make_adjoint(self, c21, inner_every=None, offload=None):
         c21 = np.asarray(c21, float).reshape(-1, 21)
         Ct = np.zeros((len(c21), 6, 6))
         for k, (i, j) in enumerate(C21_INDEX):
@@ -253,16 +374,46 @@ class Problem:
                             damped_record=self.damped_record, sponge=self.sponge,
                             damp_volume=self.damp_mask, dtype=self.dtype, device=self.device)
         solve.set_wavelet(self.wavelet)
-        return AdjointSolve(solve, self.K)
+        return AdjointSolve(solve, self.K,
+                            inner_every=self.inner_every if inner_every is None else inner_every,
+                            offload=self.offload if offload is None else offload)
 
     def traces(self, c21):
         return StiffnessTraces.fn().apply(c21, self)
 
+    def traces_numpy(self, c21):
+        """Forward traces (nt, n_groups) for the table c21, no checkpoints."""
+        c21 = np.asarray(c21, float).reshape(-1, 21)
+        Ct = np.zeros((len(c21), 6, 6))
+        for k, (i, j) in enumerate(C21_INDEX):
+            Ct[:, i, j] = c21[:, k]
+            Ct[:, j, i] = c21[:, k]
+        s_idx, s_w, r_off, r_idx, r_w = self.probe
+        solve = DeviceSolve(self.mats, Ct.reshape(-1, 36), self.rho_t, self.h, self.dt, self.coeffs,
+                            s_idx, s_w, r_off, r_idx, r_w, record=self.record,
+                            damped_record=self.damped_record, sponge=self.sponge,
+                            damp_volume=self.damp_mask, dtype=self.dtype, device=self.device)
+        try:
+            solve.set_wavelet(self.wavelet)
+            nt = len(self.wavelet)
+            solve.run(0, nt)
+            solve.check_status()
+            return np.asarray(solve.traces_numpy(nt), float)
+        finally:
+            solve.close()
+
 
 # ---------------------------------------------------------------- tables from angles
+def _host_torch():
+    """torch for the host-side angle chain (autograd on float64 CPU tensors;
+    no device is needed for it, unlike the solver)."""
+    import torch
+    return torch
+
+
 def _bond_torch(A, B):
     """Bilinear Bond form for (P,3,3) tensors; _bond_torch(R, R) = M(R)."""
-    torch = _torch()
+    torch = _host_torch()
     V = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))
     rows = []
     for (i, j) in V:
@@ -279,7 +430,7 @@ def _bond_torch(A, B):
 def rotation_colat_azim(theta, phi):
     """R = Rz(phi) Ry(theta): maps the crystal c-axis z onto
     (sin t cos p, sin t sin p, cos t)."""
-    torch = _torch()
+    torch = _host_torch()
     ct, st, cp, sp = torch.cos(theta), torch.sin(theta), torch.cos(phi), torch.sin(phi)
     z, o = torch.zeros_like(theta), torch.ones_like(theta)
     Ry = torch.stack([torch.stack([ct, z, st], -1), torch.stack([z, o, z], -1),
@@ -292,7 +443,7 @@ def rotation_colat_azim(theta, phi):
 def ice_table21(theta, phi, c_couplant=1500.0, rho_couplant=300.0, material=None):
     """(n_g + 1, 21) stiffness table (row 0 the fluid couplant) from per-grain
     c-axis angles, differentiable in theta and phi (torch float64)."""
-    torch = _torch()
+    torch = _host_torch()
     mat = ICE if material is None else material
     theta = torch.as_tensor(theta, dtype=torch.float64)
     phi = torch.as_tensor(phi, dtype=torch.float64)
@@ -328,7 +479,7 @@ def fabric_axes(params, base):
     a construction of this module (the reference's fabric fits use Watson
     (alpha, kappa) on ray-model observables, sim/model/fit_fabric.py:224-274).
     """
-    torch = _torch()
+    torch = _host_torch()
     p = torch.as_tensor(params, dtype=torch.float64)
     u = torch.as_tensor(base, dtype=torch.float64)
     s = torch.exp(p[2])
@@ -339,7 +490,7 @@ def fabric_axes(params, base):
 
 
 def theta_phi_torch(axes):
-    torch = _torch()
+    torch = _host_torch()
     z = axes[:, 2]
     sgn = torch.where(z < 0, -torch.ones_like(z), torch.ones_like(z))
     a = axes * sgn[:, None]

@@ -106,6 +106,53 @@ __device__ __forceinline__ void stg2(float *p, float a, float b)
     *reinterpret_cast<float2 *>(p) = make_float2(a, b);
 }
 __device__ __forceinline__ float pick(float2 v, int c) { return c ? v.y : v.x; }
+// Paired FP32 arithmetic (sm_100: one FADD2 / FMUL2 / FFMA2 instruction does
+// the operation on both lanes of a 64-bit register pair, each lane rounded to
+// nearest exactly as the scalar instruction). A thread's two cells share the
+// y and z offsets of every tap, so their y / z taps, the half-cell moves
+// without an x component and the update expressions run as one paired
+// instruction per operation; per lane the operations, their order and the
+// fused multiply-adds are those of the scalar code, so results are unchanged
+// bit for bit.
+__device__ __forceinline__ unsigned long long u64_of(float2 v)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2_of(unsigned long long r)
+{
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(u64_of(a)), "l"(u64_of(b)));
+    return f2_of(r);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(u64_of(a)), "l"(u64_of(b)));
+    return f2_of(r);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(u64_of(a)), "l"(u64_of(b)));
+    return f2_of(r);
+}
+// fmac2(a, b, c) = b * c + a per lane, one rounding (fmac's argument order)
+__device__ __forceinline__ float2 fmac2(float2 a, float2 b, float2 c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(u64_of(b)), "l"(u64_of(c)), "l"(u64_of(a)));
+    return f2_of(r);
+}
+
 // streaming column loads for the z rings: read once, kept out of L1 so that
 // L1 holds the material table
 __device__ __forceinline__ float2 ldg2_stream(const float *p)
@@ -131,12 +178,13 @@ __device__ __forceinline__ int lim_f(int i, int n) { return min(i + 1, n - i - 1
 template <bool G>
 __device__ __forceinline__ float tapc(float cj, int j, int lim) { return (!G || j < lim) ? cj : 0.0f; }
 
-// strain of both columns at plane q; cv = this thread's cell 0 in the vx box
+// strain of both columns at plane q; cv = this thread's cell 0 in the vx box;
+// the z rings hold both columns' values as lane pairs
 template <int NC, bool G>
 __device__ __forceinline__ void pair_strain(const StepArgs<float> &A, int q, const float *cv,
-                                            const float (&rz)[2][8], const float (&ry)[2][8],
-                                            const float (&rx)[2][8], const TapLimits &tl,
-                                            float (&g)[2][6])
+                                            const float2 (&rz)[8], const float2 (&ry)[8],
+                                            const float2 (&rx)[8], const TapLimits &tl,
+                                            float2 (&g)[6])
 {
     constexpr int W = PS_VW;
     const float *tvx = cv, *tvy = cv + PS_VSZ, *tvz = cv + 2 * PS_VSZ;
@@ -148,8 +196,7 @@ __device__ __forceinline__ void pair_strain(const StepArgs<float> &A, int q, con
         Y[2 * k] = b.x; Y[2 * k + 1] = b.y;
         Z[2 * k] = c.x; Z[2 * k + 1] = c.y;
     }
-    float a1[2] = {0.f, 0.f}, a2[2] = {0.f, 0.f}, a3[2] = {0.f, 0.f};
-    float a4[2] = {0.f, 0.f}, a5[2] = {0.f, 0.f}, a6[2] = {0.f, 0.f};
+    float2 a1 = bc2(0.f), a2 = bc2(0.f), a3 = bc2(0.f), a4 = bc2(0.f), a5 = bc2(0.f), a6 = bc2(0.f);
     const int nz = A.nz;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -157,36 +204,42 @@ __device__ __forceinline__ void pair_strain(const StepArgs<float> &A, int q, con
             const float cj = A.c[j];
             const float czb = tapc<G>(cj, j, lim_b(q, nz)), czf = tapc<G>(cj, j, lim_f(q, nz));
             const float cyb = tapc<G>(cj, j, tl.yb), cyf = tapc<G>(cj, j, tl.yf);
+            const float cxb0 = tapc<G>(cj, j, tl.xb[0]), cxb1 = tapc<G>(cj, j, tl.xb[1]);
+            const float cxf0 = tapc<G>(cj, j, tl.xf[0]), cxf1 = tapc<G>(cj, j, tl.xf[1]);
             const float2 yp = lds2(tvy + j * W), ym = lds2(tvy - (j + 1) * W);     // Dby vy
             const float2 zp = lds2(tvz + (j + 1) * W), zm = lds2(tvz - j * W);     // Dfy vz
             const float2 xp = lds2(tvx + (j + 1) * W), xm = lds2(tvx - j * W);     // Dfy vx
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const float cxb = tapc<G>(cj, j, tl.xb[c]), cxf = tapc<G>(cj, j, tl.xf[c]);
-                a1[c] = fmac(a1[c], cxb, X[4 + c + j] - X[3 + c - j]);
-                a2[c] = fmac(a2[c], cyb, pick(yp, c) - pick(ym, c));
-                a3[c] = fmac(a3[c], czb, rz[c][4 + j] - rz[c][3 - j]);
-                a4[c] = fmac(a4[c], cyf, pick(zp, c) - pick(zm, c));
-                a4[c] = fmac(a4[c], czf, ry[c][4 + j] - ry[c][3 - j]);
-                a5[c] = fmac(a5[c], cxf, Z[5 + c + j] - Z[4 + c - j]);
-                a5[c] = fmac(a5[c], czf, rx[c][4 + j] - rx[c][3 - j]);
-                a6[c] = fmac(a6[c], cxf, Y[5 + c + j] - Y[4 + c - j]);
-                a6[c] = fmac(a6[c], cyf, pick(xp, c) - pick(xm, c));
-            }
+            // per lane: a1 x; a2 y; a3 z; a4 y, z; a5 x, z; a6 x, y
+            a1.x = fmac(a1.x, cxb0, X[4 + j] - X[3 - j]);
+            a1.y = fmac(a1.y, cxb1, X[5 + j] - X[4 - j]);
+            a2 = fmac2(a2, bc2(cyb), sub2(yp, ym));
+            a3 = fmac2(a3, bc2(czb), sub2(rz[4 + j], rz[3 - j]));
+            a4 = fmac2(a4, bc2(cyf), sub2(zp, zm));
+            a4 = fmac2(a4, bc2(czf), sub2(ry[4 + j], ry[3 - j]));
+            a5.x = fmac(a5.x, cxf0, Z[5 + j] - Z[4 - j]);
+            a5.y = fmac(a5.y, cxf1, Z[6 + j] - Z[5 - j]);
+            a5 = fmac2(a5, bc2(czf), sub2(rx[4 + j], rx[3 - j]));
+            a6.x = fmac(a6.x, cxf0, Y[5 + j] - Y[4 - j]);
+            a6.y = fmac(a6.y, cxf1, Y[6 + j] - Y[5 - j]);
+            a6 = fmac2(a6, bc2(cyf), sub2(xp, xm));
         }
     }
-    const float ih = A.inv_h;
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        g[c][0] = a1[c] * ih; g[c][1] = a2[c] * ih; g[c][2] = a3[c] * ih;
-        g[c][3] = a4[c] * ih; g[c][4] = a5[c] * ih; g[c][5] = a6[c] * ih;
-    }
+    const float2 ih = bc2(A.inv_h);
+    g[0] = mul2(a1, ih); g[1] = mul2(a2, ih); g[2] = mul2(a3, ih);
+    g[3] = mul2(a4, ih); g[4] = mul2(a5, ih); g[5] = mul2(a6, ih);
 }
 
 // strain J at (dz, dy) and column offset dx in -1..2 from cell 0. pl[0]:
 // the 4-plane ring slot of plane z - 1, pl[1] of z (both at this thread's
 // cell 0, component offsets added here); pl[2]: the 3-plane ring slot of
 // z, pl[3] of z + 1.
+// address of the lane pair (cell 0, cell 1) of strain J at (dz, dy), column
+// offset 0
+__device__ __forceinline__ const float *gptr(const float *const (&pl)[4], int J, int dz, int dy)
+{
+    const float *b = (J == 3 || J == 4) ? pl[dz + 1] : pl[dz + 2];
+    return b + ring_base(J) * PS_GST + dy * PS_GW;
+}
 __device__ __forceinline__ float gval(const float *const (&pl)[4], int J, int dz, int dy, int dx)
 {
     const float *b = (J == 3 || J == 4) ? pl[dz + 1] : pl[dz + 2];
@@ -201,20 +254,42 @@ struct MoveGuards {
 
 // strain J moved to position P (sim/core/fdtd.py:612-633) for both cells:
 // 4 taps summed z-major, times 1/4, zero where a needed neighbour is off
-// the grid; the term order of qval() in pe_kernels.cuh
+// the grid; the term order of qval() in pe_kernels.cuh. A move without an x
+// component reads the same column offsets for both cells (one 64-bit load
+// per tap, paired sums); the others combine lanes per cell.
 template <int P, int J, bool G>
-__device__ __forceinline__ void qpair(const float *const (&pl)[4], const MoveGuards &mg, float (&q)[2])
+__device__ __forceinline__ void qpair(const float *const (&pl)[4], const MoveGuards &mg, float2 &q)
 {
     constexpr int S = vpos(J);
     constexpr int DZ = pos_z(P) - pos_z(S), DY = pos_y(P) - pos_y(S), DX = pos_x(P) - pos_x(S);
+    constexpr int LZ = DZ < 0 ? -1 : 0, HZ = DZ > 0 ? 1 : 0;
+    constexpr int LY = DY < 0 ? -1 : 0, HY = DY > 0 ? 1 : 0;
+    if constexpr (DZ == 0 && DY == 0 && DX == 0) {
+        q = lds2(gptr(pl, J, 0, 0));
+    } else if constexpr (DX == 0) {
+        float2 acc = bc2(0.f);
+        bool first = true;
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        if constexpr (DZ == 0 && DY == 0 && DX == 0) {
-            q[c] = gval(pl, J, 0, 0, c);
-        } else {
-            constexpr int LZ = DZ < 0 ? -1 : 0, HZ = DZ > 0 ? 1 : 0;
-            constexpr int LY = DY < 0 ? -1 : 0, HY = DY > 0 ? 1 : 0;
-            constexpr int LX = DX < 0 ? -1 : 0, HX = DX > 0 ? 1 : 0;
+        for (int a0 = LZ; a0 <= HZ; ++a0)
+#pragma unroll
+            for (int a1 = LY; a1 <= HY; ++a1) {
+                const float2 t = lds2(gptr(pl, J, a0, a1));
+                acc = first ? t : add2(acc, t);
+                first = false;
+            }
+        bool ok = true;
+        if constexpr (G) {
+            if constexpr (DZ > 0) ok = ok && mg.zhi;
+            if constexpr (DZ < 0) ok = ok && mg.zlo;
+            if constexpr (DY > 0) ok = ok && mg.yhi;
+            if constexpr (DY < 0) ok = ok && mg.ylo;
+        }
+        q = ok ? mul2(acc, bc2(0.25f)) : bc2(0.0f);
+    } else {
+        constexpr int LX = DX < 0 ? -1 : 0, HX = DX > 0 ? 1 : 0;
+        float r[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
             float acc = 0.f;
             bool first = true;
 #pragma unroll
@@ -235,45 +310,56 @@ __device__ __forceinline__ void qpair(const float *const (&pl)[4], const MoveGua
                 if constexpr (DY < 0) ok = ok && mg.ylo;
                 if constexpr (DX > 0) ok = ok && mg.xhi[c];
                 if constexpr (DX < 0) ok = ok && mg.xlo[c];
-                q[c] = ok ? acc * 0.25f : 0.0f;
+                r[c] = ok ? acc * 0.25f : 0.0f;
             } else {
-                q[c] = acc * 0.25f;
+                r[c] = acc * 0.25f;
             }
         }
+        q = make_float2(r[0], r[1]);
     }
 }
 
 // column J of the stiffness product: acc[I] = fmac(acc[I], C[I][J], q_J at
 // the position of stress I), J ascending as in row_dot(). TS: the table is
-// in shared memory (else global, through the read-only cache).
+// in shared memory (else global, through the read-only cache). The two cells
+// hold different materials, so these run per lane.
 template <int J, bool G, bool TS>
 __device__ __forceinline__ void stiff_column(const float *const (&pl)[4], const MoveGuards &mg,
-                                             const float *const (&crow)[2], float (&acc)[6][2])
+                                             const float *const (&crow)[2], float2 (&acc)[6])
 {
-    float q0[2], q1[2], q2[2], q3[2];
+    float2 q0, q1, q2, q3;
     qpair<0, J, G>(pl, mg, q0);
     qpair<1, J, G>(pl, mg, q1);
     qpair<2, J, G>(pl, mg, q2);
     qpair<3, J, G>(pl, mg, q3);
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        const float4 a = TS ? lds4(crow[c] + 4 * J) : ldg4(crow[c] + 4 * J);
-        const float2 b = TS ? lds2(crow[c] + 24 + 2 * J) : ldg2(crow[c] + 24 + 2 * J);
-        acc[0][c] = fmac(acc[0][c], a.x, q0[c]);
-        acc[1][c] = fmac(acc[1][c], a.y, q0[c]);
-        acc[2][c] = fmac(acc[2][c], a.z, q0[c]);
-        acc[3][c] = fmac(acc[3][c], a.w, q1[c]);
-        acc[4][c] = fmac(acc[4][c], b.x, q2[c]);
-        acc[5][c] = fmac(acc[5][c], b.y, q3[c]);
+    {
+        const float4 a = TS ? lds4(crow[0] + 4 * J) : ldg4(crow[0] + 4 * J);
+        const float2 b = TS ? lds2(crow[0] + 24 + 2 * J) : ldg2(crow[0] + 24 + 2 * J);
+        acc[0].x = fmac(acc[0].x, a.x, q0.x);
+        acc[1].x = fmac(acc[1].x, a.y, q0.x);
+        acc[2].x = fmac(acc[2].x, a.z, q0.x);
+        acc[3].x = fmac(acc[3].x, a.w, q1.x);
+        acc[4].x = fmac(acc[4].x, b.x, q2.x);
+        acc[5].x = fmac(acc[5].x, b.y, q3.x);
+    }
+    {
+        const float4 a = TS ? lds4(crow[1] + 4 * J) : ldg4(crow[1] + 4 * J);
+        const float2 b = TS ? lds2(crow[1] + 24 + 2 * J) : ldg2(crow[1] + 24 + 2 * J);
+        acc[0].y = fmac(acc[0].y, a.x, q0.y);
+        acc[1].y = fmac(acc[1].y, a.y, q0.y);
+        acc[2].y = fmac(acc[2].y, a.z, q0.y);
+        acc[3].y = fmac(acc[3].y, a.w, q1.y);
+        acc[4].y = fmac(acc[4].y, b.x, q2.y);
+        acc[5].y = fmac(acc[5].y, b.y, q3.y);
     }
 }
 
 template <bool G, bool TS>
 __device__ __forceinline__ void stiff_all(const float *const (&pl)[4], const MoveGuards &mg,
-                                          const float *const (&crow)[2], float (&acc)[6][2])
+                                          const float *const (&crow)[2], float2 (&acc)[6])
 {
 #pragma unroll
-    for (int I = 0; I < 6; ++I) acc[I][0] = acc[I][1] = 0.f;
+    for (int I = 0; I < 6; ++I) acc[I] = bc2(0.f);
     stiff_column<0, G, TS>(pl, mg, crow, acc);
     stiff_column<1, G, TS>(pl, mg, crow, acc);
     stiff_column<2, G, TS>(pl, mg, crow, acc);
@@ -366,13 +452,12 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     auto ld2col = [&](const float *f, int q) -> float2 {
         return (pair_ok && q >= 0 && q < nz) ? ldg2_stream(f + (long long)q * sz) : make_float2(0.f, 0.f);
     };
-    float rz[2][8], ry[2][8], rx[2][8];
+    float2 rz[8], ry[8], rx[8];   // lane pairs (cell 0, cell 1)
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const float2 a = ld2col(pz, q0 - 4 + k), b = ld2col(py, q0 - 3 + k), c = ld2col(px, q0 - 3 + k);
-        rz[0][k] = a.x; rz[1][k] = a.y;
-        ry[0][k] = b.x; ry[1][k] = b.y;
-        rx[0][k] = c.x; rx[1][k] = c.y;
+        rz[k] = ld2col(pz, q0 - 4 + k);
+        ry[k] = ld2col(py, q0 - 3 + k);
+        rx[k] = ld2col(px, q0 - 3 + k);
     }
     TapLimits tl;
     MoveGuards mg;
@@ -436,26 +521,23 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
         const bool fast = NC == 4 && TIN && q >= T_H && q <= nz - 1 - T_H;
         if (warp_rows_in) {
             const float *tv = vslot + cv;
-            float g[2][6];
+            float2 g[6];
             if (fast) pair_strain<NC, false>(A, q, tv, rz, ry, rx, tl, g);
             else pair_strain<NC, true>(A, q, tv, rz, ry, rx, tl, g);
             const int s4 = q & 3;   // ring slots of plane q: r3 and q mod 4
 #pragma unroll
             for (int J = 0; J < 6; ++J)
-                stg2(gs + (ring_base(J) + (ring_planes(J) == 4 ? s4 : r3)) * PS_GST + cg, g[0][J], g[1][J]);
+                *reinterpret_cast<float2 *>(gs + (ring_base(J) + (ring_planes(J) == 4 ? s4 : r3)) * PS_GST + cg) = g[J];
         }
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                rz[c][k] = rz[c][k + 1];
-                ry[c][k] = ry[c][k + 1];
-                rx[c][k] = rx[c][k + 1];
-            }
+            rz[k] = rz[k + 1];
+            ry[k] = ry[k + 1];
+            rx[k] = rx[k + 1];
         }
-        rz[0][7] = nzv.x; rz[1][7] = nzv.y;
-        ry[0][7] = nyv.x; ry[1][7] = nyv.y;
-        rx[0][7] = nxv.x; rx[1][7] = nxv.y;
+        rz[7] = nzv;
+        ry[7] = nyv;
+        rx[7] = nxv;
         // the cell boxes of plane z (issued a plane earlier): warp 7, which
         // has no cell to update, waits for them before the block barrier,
         // and the barrier orders every other warp's reads after that wait
@@ -475,7 +557,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
             mg.zhi = z <= nz - 2;
             const uint16_t lab[2] = {(uint16_t)(lab2 & 0xFFFFu), (uint16_t)(lab2 >> 16)};
             const float *const crow[2] = {tab + (lab[0] & LAB_MAT) * TAB36, tab + (lab[1] & LAB_MAT) * TAB36};
-            float acc[6][2];
+            float2 acc[6];
             if (fast) stiff_all<false, TS>(pl, mg, crow, acc);
             else stiff_all<true, TS>(pl, mg, crow, acc);
             const float *sc = sslots + (us & 1) * PS_SSLOT + cs;
@@ -495,12 +577,14 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
                     dmp[c] = d;
                 }
             }
+            // s = fmac(s_old * damp, dt, acc) per lane
+            const float2 dmp2 = make_float2(dmp[0], dmp[1]), dt2 = bc2(A.dt);
             float sv[6][2];
 #pragma unroll
             for (int I = 0; I < 6; ++I) {
-                const float2 so = lds2(sc + I * PS_SSZP);
-                sv[I][0] = fmac(so.x * dmp[0], A.dt, acc[I][0]);
-                sv[I][1] = fmac(so.y * dmp[1], A.dt, acc[I][1]);
+                const float2 v = fmac2(mul2(lds2(sc + I * PS_SSZP), dmp2), dt2, acc[I]);
+                sv[I][0] = v.x;
+                sv[I][1] = v.y;
             }
             const long long idx0 = (long long)z * sz + col;
 #pragma unroll
@@ -693,10 +777,10 @@ __global__ void k_rho_inv(const float *rho, float *rinv, int n_mat)
 template <int NC, bool G>
 __device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, const float *t1,
                                               const float *t2, const float *t4, const float *t5,
-                                              const float *t6, const float (&r3)[2][8],
-                                              const float (&r4)[2][8], const float (&r5)[2][8],
-                                              const TapLimits &tl, float (&ax)[2], float (&ay)[2],
-                                              float (&az)[2])
+                                              const float *t6, const float2 (&r3)[8],
+                                              const float2 (&r4)[8], const float2 (&r5)[8],
+                                              const TapLimits &tl, float2 &ax, float2 &ay,
+                                              float2 &az)
 {
     constexpr int W = PV_TW;
     float S1[10], S5[10], S6[10];   // centre rows, columns (cell 0) - 4 .. + 5
@@ -708,8 +792,7 @@ __device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, c
         S6[2 * k] = c.x; S6[2 * k + 1] = c.y;
     }
     const int nz = A.nz;
-#pragma unroll
-    for (int c = 0; c < 2; ++c) ax[c] = ay[c] = az[c] = 0.f;
+    ax = ay = az = bc2(0.f);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (NC ? j < NC : j < A.nc) {
@@ -719,19 +802,21 @@ __device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, c
             const float2 p4 = lds2(t4 + j * W), m4 = lds2(t4 - (j + 1) * W);         // Dby s4
             const float czf = tapc<G>(cj, j, lim_f(z, nz)), czb = tapc<G>(cj, j, lim_b(z, nz));
             const float cyf = tapc<G>(cj, j, tl.yf), cyb = tapc<G>(cj, j, tl.yb);
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const float cxb = tapc<G>(cj, j, tl.xb[c]), cxf = tapc<G>(cj, j, tl.xf[c]);
-                ax[c] = fmac(ax[c], cxf, S1[5 + c + j] - S1[4 + c - j]);
-                ay[c] = fmac(ay[c], cxb, S6[4 + c + j] - S6[3 + c - j]);
-                az[c] = fmac(az[c], cxb, S5[4 + c + j] - S5[3 + c - j]);
-                ay[c] = fmac(ay[c], cyf, pick(p2, c) - pick(m2, c));
-                ax[c] = fmac(ax[c], cyb, pick(p6, c) - pick(m6, c));
-                az[c] = fmac(az[c], cyb, pick(p4, c) - pick(m4, c));
-                az[c] = fmac(az[c], czf, r3[c][4 + j] - r3[c][3 - j]);
-                ax[c] = fmac(ax[c], czb, r5[c][4 + j] - r5[c][3 - j]);
-                ay[c] = fmac(ay[c], czb, r4[c][4 + j] - r4[c][3 - j]);
-            }
+            const float cxb0 = tapc<G>(cj, j, tl.xb[0]), cxb1 = tapc<G>(cj, j, tl.xb[1]);
+            const float cxf0 = tapc<G>(cj, j, tl.xf[0]), cxf1 = tapc<G>(cj, j, tl.xf[1]);
+            // per lane: x taps, then y, then z, for each of ax, ay, az
+            ax.x = fmac(ax.x, cxf0, S1[5 + j] - S1[4 - j]);
+            ax.y = fmac(ax.y, cxf1, S1[6 + j] - S1[5 - j]);
+            ay.x = fmac(ay.x, cxb0, S6[4 + j] - S6[3 - j]);
+            ay.y = fmac(ay.y, cxb1, S6[5 + j] - S6[4 - j]);
+            az.x = fmac(az.x, cxb0, S5[4 + j] - S5[3 - j]);
+            az.y = fmac(az.y, cxb1, S5[5 + j] - S5[4 - j]);
+            ay = fmac2(ay, bc2(cyf), sub2(p2, m2));
+            ax = fmac2(ax, bc2(cyb), sub2(p6, m6));
+            az = fmac2(az, bc2(cyb), sub2(p4, m4));
+            az = fmac2(az, bc2(czf), sub2(r3[4 + j], r3[3 - j]));
+            ax = fmac2(ax, bc2(czb), sub2(r5[4 + j], r5[3 - j]));
+            ay = fmac2(ay, bc2(czb), sub2(r4[4 + j], r4[3 - j]));
         }
     }
 }
@@ -783,13 +868,12 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
     auto ld2col = [&](const float *f, int z) -> float2 {
         return (out_ok && z >= 0 && z < nz) ? ldg2_stream(f + (long long)z * sz) : make_float2(0.f, 0.f);
     };
-    float r3[2][8], r4[2][8], r5[2][8];   // r3[c][k] <-> z-3+k, r4/r5[c][k] <-> z-4+k
+    float2 r3[8], r4[8], r5[8];   // lane pairs: r3[k] <-> z-3+k, r4/r5[k] <-> z-4+k
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const float2 a = ld2col(p3, zb - 3 + k), b = ld2col(p4, zb - 4 + k), c = ld2col(p5, zb - 4 + k);
-        r3[0][k] = a.x; r3[1][k] = a.y;
-        r4[0][k] = b.x; r4[1][k] = b.y;
-        r5[0][k] = c.x; r5[1][k] = c.y;
+        r3[k] = ld2col(p3, zb - 3 + k);
+        r4[k] = ld2col(p4, zb - 4 + k);
+        r5[k] = ld2col(p5, zb - 4 + k);
     }
     TapLimits tl;
     if constexpr (TIN) {
@@ -844,7 +928,7 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
         ldlabs(z + 2, mlab_c, mlab_x2, mlab_y);
         const float *slot = slots + sl * PV_SLOT;
         const float *t = slot + tc;
-        float ax[2], ay[2], az[2];
+        float2 ax, ay, az;
         const bool fast = NC == 4 && TIN && z >= T_H && z <= nz - 1 - T_H;
         if (fast) pair_vel_taps<NC, false>(A, z, t, t + PV_TSZ, t + 2 * PV_TSZ, t + 3 * PV_TSZ, t + 4 * PV_TSZ, r3, r4, r5, tl, ax, ay, az);
         else pair_vel_taps<NC, true>(A, z, t, t + PV_TSZ, t + 2 * PV_TSZ, t + 3 * PV_TSZ, t + 4 * PV_TSZ, r3, r4, r5, tl, ax, ay, az);
@@ -870,44 +954,56 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
                     dmp[c] = d;
                 }
             }
-            const float2 vxo = lds2(vc), vyo = lds2(vc + PV_CSZ), vzo = lds2(vc + 2 * PV_CSZ);
+            const float2 vo[3] = {lds2(vc), lds2(vc + PV_CSZ), lds2(vc + 2 * PV_CSZ)};
             // the six face divisions: Markstein quotients for all of them
-            // (independent chains), then the exact fallback for the lanes
-            // whose numerator or face rules that out (div_face_rcp)
-            float u[2][3], rv[2][3], yr[2], q[2][3];
-            bool fine = true;
+            // (independent chains, lane pairs), then the exact fallback for
+            // the lanes whose numerator or face rules that out (div_face_rcp)
+            float r0[2], rn[2][3];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const bool xin = c == 0 ? true : xin1;
-                const float r0 = rho_tab[lc[c] & LAB_MAT];
-                yr[c] = __ldg(A.rinv + (lc[c] & LAB_MAT));
-                rv[c][0] = xin ? 0.5f * (r0 + rho_tab[lxv[c] & LAB_MAT]) : r0;
-                rv[c][1] = yin ? 0.5f * (r0 + rho_tab[lyv[c] & LAB_MAT]) : r0;
-                rv[c][2] = (z < nz - 1) ? 0.5f * (r0 + rho_tab[lzv[c] & LAB_MAT]) : r0;
-                u[c][0] = A.dt_h * ax[c];
-                u[c][1] = A.dt_h * ay[c];
-                u[c][2] = A.dt_h * az[c];
+                r0[c] = rho_tab[lc[c] & LAB_MAT];
+                rn[c][0] = xin ? rho_tab[lxv[c] & LAB_MAT] : 0.f;
+                rn[c][1] = yin ? rho_tab[lyv[c] & LAB_MAT] : 0.f;
+                rn[c][2] = (z < nz - 1) ? rho_tab[lzv[c] & LAB_MAT] : 0.f;
+            }
+            const bool has_nb[2][3] = {{true, yin, z < nz - 1}, {xin1, yin, z < nz - 1}};
+            const float2 r02 = make_float2(r0[0], r0[1]);
+            const float2 y2 = make_float2(__ldg(A.rinv + (lc[0] & LAB_MAT)), __ldg(A.rinv + (lc[1] & LAB_MAT)));
+            const float2 a2[3] = {ax, ay, az};
+            float2 u[3], rv[3], q[3];
+            bool fine = true;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    q[c][d] = markstein(u[c][d], rv[c][d], yr[c]);
-                    const float au = fabsf(u[c][d]);
-                    fine = fine && rv[c][d] == r0 && au >= 0x1p-100f && au <= 0x1p100f;
+            for (int d = 0; d < 3; ++d) {
+                // face density 0.5 (rho0 + rho1), or the cell's own at the last slice
+                const float2 h = mul2(bc2(0.5f), add2(r02, make_float2(rn[0][d], rn[1][d])));
+                rv[d] = make_float2(has_nb[0][d] ? h.x : r0[0], has_nb[1][d] ? h.y : r0[1]);
+                u[d] = mul2(bc2(A.dt_h), a2[d]);
+                // markstein(u, rv, y) per lane: q0 = u y, two corrections
+                const float2 nb = make_float2(-rv[d].x, -rv[d].y);
+                const float2 q0 = mul2(u[d], y2);
+                const float2 q1 = fmac2(q0, fmac2(u[d], nb, q0), y2);
+                q[d] = fmac2(q1, fmac2(u[d], nb, q1), y2);
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float au = fabsf(c ? u[d].y : u[d].x);
+                    fine = fine && (c ? rv[d].y : rv[d].x) == r0[c] && au >= 0x1p-100f && au <= 0x1p100f;
                 }
             }
             if (!fine) {
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const float r0 = rho_tab[lc[c] & LAB_MAT];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) q[c][d] = div_face_rcp(u[c][d], rv[c][d], rv[c][d] == r0, yr[c]);
+                for (int d = 0; d < 3; ++d) {
+                    q[d].x = div_face_rcp(u[d].x, rv[d].x, rv[d].x == r0[0], y2.x);
+                    q[d].y = div_face_rcp(u[d].y, rv[d].y, rv[d].y == r0[1], y2.y);
                 }
             }
+            const float2 dmp2 = make_float2(dmp[0], dmp[1]);
             float vn[3][2];
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                vn[0][c] = (pick(vxo, c) + q[c][0]) * dmp[c];
-                vn[1][c] = (pick(vyo, c) + q[c][1]) * dmp[c];
-                vn[2][c] = (pick(vzo, c) + q[c][2]) * dmp[c];
+            for (int d = 0; d < 3; ++d) {
+                const float2 v = mul2(add2(vo[d], q[d]), dmp2);
+                vn[d][0] = v.x;
+                vn[d][1] = v.y;
             }
             const long long idx = (long long)z * sz + col;
             stg2(A.v[0] + idx, vn[0][0], vn[0][1]);
@@ -924,16 +1020,13 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
         nlab_c = mlab_c; nlab_x2 = mlab_x2; nlab_y = mlab_y;
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                r3[c][k] = r3[c][k + 1];
-                r4[c][k] = r4[c][k + 1];
-                r5[c][k] = r5[c][k + 1];
-            }
+            r3[k] = r3[k + 1];
+            r4[k] = r4[k + 1];
+            r5[k] = r5[k + 1];
         }
-        r3[0][7] = n3.x; r3[1][7] = n3.y;
-        r4[0][7] = n4.x; r4[1][7] = n4.y;
-        r5[0][7] = n5.x; r5[1][7] = n5.y;
+        r3[7] = n3;
+        r4[7] = n4;
+        r5[7] = n5;
     }
     return ze - zb;
 }

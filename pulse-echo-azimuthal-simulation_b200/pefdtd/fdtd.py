@@ -86,7 +86,9 @@ def c_solve_structs(mats, Ct, rho_t, h, dt, coeffs, src_idx, src_w, rec_off, rec
     until the solver has been created."""
     torch = _torch()
     npdt, pedt = _dtype(dtype)
-    mats = np.asarray(mats)
+    on_device = isinstance(mats, torch.Tensor)   # material indices already on the device
+    if not on_device:
+        mats = np.asarray(mats)
     shape = tuple(int(v) for v in mats.shape)
     nz, ny, nx = shape
     coeffs = np.asarray(coeffs, float).reshape(-1)
@@ -112,7 +114,11 @@ def c_solve_structs(mats, Ct, rho_t, h, dt, coeffs, src_idx, src_w, rec_off, rec
     cfg.variant = _capi.KERNEL_VARIANT[variant]
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     with torch.cuda.device(dev):
-        lab_t = torch.from_numpy(np.ascontiguousarray(mats.astype(np.uint16).view(np.int16))).to(dev)
+        if on_device:
+            # indices below 2^14 (the flag bits are set by the solver): int16 holds them
+            lab_t = mats.to(device=dev, dtype=torch.int16).contiguous()
+        else:
+            lab_t = torch.from_numpy(np.ascontiguousarray(mats.astype(np.uint16).view(np.int16))).to(dev)
         dvol_t = (torch.from_numpy(np.ascontiguousarray(damp_volume, np.float32)).to(dev)
                   if damp_volume is not None else None)
     keep = [lab_t, dvol_t, Ct, rho_t]
