@@ -77,7 +77,15 @@ typedef struct PeConfig {
  * one-column tiled kernels. COLUMN forces the one-column tiled kernels and
  * SIMPLE the untiled ones (every tap read through the L1 cache); both are
  * kept as independent cross-checks of TILED. */
-enum PeKernelVariant { PE_KERNEL_TILED = 0, PE_KERNEL_SIMPLE = 1, PE_KERNEL_COLUMN = 2 };
+enum PeKernelVariant { PE_KERNEL_TILED = 0, PE_KERNEL_SIMPLE = 1, PE_KERNEL_COLUMN = 2, PE_KERNEL_DENSE = 3 };
+/* PE_KERNEL_DENSE: per-cell media, the reference's dense path (forward_fused
+ * with 21 arbitrary stiffness maps, sim/core/fdtd.py:831-921, kernels K1-K3
+ * :392-583): the medium tables hold one row per cell (n_mat == nz * ny * nx,
+ * row i for the cell of linear index i; PE_MAX_MATERIALS does not apply),
+ * labels_dev is not read (may be NULL). Runs the untiled kernels with the
+ * row looked up by cell index; same arithmetic, so a medium that also fits a
+ * table gives bit-identical results either way. Not available to batches or
+ * the adjoint. */
 
 /* The medium. Volumes live on the device; tables are small host arrays. */
 typedef struct PeMedium {

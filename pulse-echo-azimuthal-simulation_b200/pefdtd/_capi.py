@@ -27,7 +27,7 @@ class PeConfig(C.Structure):
                 ("variant", C.c_int32)]
 
 
-KERNEL_VARIANT = {"tiled": 0, "simple": 1, "column": 2}
+KERNEL_VARIANT = {"tiled": 0, "simple": 1, "column": 2, "dense": 3}
 
 
 class PeMedium(C.Structure):

@@ -67,6 +67,7 @@ struct StepArgs {
     int k;                      // step within the chunk
     int zc;                     // planes per z-march
     int *status;                // device status word (bounded waits record timeouts)
+    int dense;                  // per-cell media: the table row of cell i is i (untiled kernels)
 };
 
 // ---------------------------------------------------------------- helpers
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(TX *TY) k_stress(const StepArgs<T> A)
 
             const long long idx = z * A.sz + iy * A.sy + ix;
             const uint16_t lab = A.lab[idx];
-            const T *Cr = A.c21 + (long long)(lab & LAB_MAT) * C21_STRIDE;
+            const T *Cr = A.c21 + (A.dense ? idx : (long long)(lab & LAB_MAT)) * C21_STRIDE;
             T Cm[21];
 #pragma unroll
             for (int k = 0; k < 21; ++k) Cm[k] = ldg(Cr + k);
@@ -377,10 +378,14 @@ __global__ void __launch_bounds__(TX *TY) k_velocity(const StepArgs<T> A)
             }
         }
         const uint16_t lab = A.lab[idx];
-        const T r0 = ldg(A.rho + (lab & LAB_MAT));
-        const T rvx = (ix < nx - 1) ? T(0.5) * (r0 + ldg(A.rho + (A.lab[idx + 1] & LAB_MAT))) : r0;
-        const T rvy = (iy < ny - 1) ? T(0.5) * (r0 + ldg(A.rho + (A.lab[idx + sy] & LAB_MAT))) : r0;
-        const T rvz = (iz < nz - 1) ? T(0.5) * (r0 + ldg(A.rho + (A.lab[idx + sz] & LAB_MAT))) : r0;
+        // density of a cell: its table row (the cell itself for per-cell media)
+        auto rho_at = [&](long long q) -> T {
+            return ldg(A.rho + (A.dense ? q : (long long)(A.lab[q] & LAB_MAT)));
+        };
+        const T r0 = rho_at(idx);
+        const T rvx = (ix < nx - 1) ? T(0.5) * (r0 + rho_at(idx + 1)) : r0;
+        const T rvy = (iy < ny - 1) ? T(0.5) * (r0 + rho_at(idx + sy)) : r0;
+        const T rvz = (iz < nz - 1) ? T(0.5) * (r0 + rho_at(idx + sz)) : r0;
         const T dmp = (T)damp_at(A, iz, iy, ix, idx);
         T tx = A.dt_h * ax, ty = A.dt_h * ay, tz = A.dt_h * az;
         tx = div_face(tx, rvx); ty = div_face(ty, rvy); tz = div_face(tz, rvz);

@@ -166,6 +166,7 @@ pe::StepArgs<T> make_args(const PeSolver *S, const PeState *st, int k)
     A.k = k;
     A.zc = S->zc_s;
     A.status = S->status;
+    A.dense = S->variant == PE_KERNEL_DENSE;
     return A;
 }
 
@@ -187,7 +188,7 @@ void launch_simple_velocity(pe::StepArgs<T> A, int zc, cudaStream_t st)
 template <typename T>
 void launch_stress(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st)
 {
-    if (S->variant == PE_KERNEL_SIMPLE) {
+    if (S->variant == PE_KERNEL_SIMPLE || S->variant == PE_KERNEL_DENSE) {
         if (S->ty == 8) launch_simple_stress<T, 32, 8>(A0, S->zc_s, st);
         else launch_simple_stress<T, 32, 4>(A0, S->zc_s, st);
         return;
@@ -223,7 +224,7 @@ void launch_stress(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st
 template <typename T>
 void launch_velocity(const PeSolver *S, const pe::StepArgs<T> &A0, cudaStream_t st)
 {
-    if (S->variant == PE_KERNEL_SIMPLE) {
+    if (S->variant == PE_KERNEL_SIMPLE || S->variant == PE_KERNEL_DENSE) {
         if (S->ty == 8) launch_simple_velocity<T, 32, 8>(A0, S->zc_v, st);
         else launch_simple_velocity<T, 32, 4>(A0, S->zc_v, st);
         return;
@@ -364,7 +365,7 @@ template <typename T>
 int configure_kernels(PeSolver *S)
 {
     const PeConfig &c = S->cfg;
-    if (S->variant == PE_KERNEL_SIMPLE) {
+    if (S->variant == PE_KERNEL_SIMPLE || S->variant == PE_KERNEL_DENSE) {
         const long long tiles = (long long)((c.nx + S->tx - 1) / S->tx) * ((c.ny + S->ty - 1) / S->ty);
         const int slots = occupancy_slots(pe::k_stress<T, 32, 8>, 32 * S->ty, 0);
         S->zc_s = c.z_chunk > 0 ? c.z_chunk : pick_zchunk(c.nz, tiles, slots, 2);
@@ -506,10 +507,14 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
                         " coefficients given): the kernels carry +/-4 taps per axis");
     if (c.dtype != PE_F32 && c.dtype != PE_F64) return fail(PE_ERR_INVALID, "dtype must be F32 or F64");
     if (c.record < 0 || c.record > 3) return fail(PE_ERR_INVALID, "record must be 0..3");
-    if (c.n_mat < 1 || c.n_mat > PE_MAX_MATERIALS)
+    const bool dense = c.variant == PE_KERNEL_DENSE;
+    if (dense && (long long)c.n_mat != (long long)c.nz * c.ny * c.nx)
+        return fail(PE_ERR_INVALID, "per-cell media (PE_KERNEL_DENSE) need one table row per cell: n_mat = " +
+                                        std::to_string((long long)c.nz * c.ny * c.nx));
+    if (!dense && (c.n_mat < 1 || c.n_mat > PE_MAX_MATERIALS))
         return fail(PE_ERR_INVALID, "n_mat must lie in [1, " + std::to_string(PE_MAX_MATERIALS) + "]");
     if (!(c.h > 0) || !(c.dt > 0)) return fail(PE_ERR_INVALID, "h and dt must be positive");
-    if (!md->labels_dev || !md->ctab || !md->rho)
+    if ((!dense && !md->labels_dev) || !md->ctab || !md->rho)
         return fail(PE_ERR_INVALID, "labels_dev, ctab and rho are required");
     const bool any_sp = md->sponge_z || md->sponge_y || md->sponge_x;
     const bool all_sp = md->sponge_z && md->sponge_y && md->sponge_x;
@@ -524,14 +529,16 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     S->ncell = (long long)c.nz * c.ny * c.nx;
     S->esize = dtype_size(c.dtype);
     S->chunk = c.chunk_steps > 0 ? c.chunk_steps : 200;
-    if (c.variant != PE_KERNEL_TILED && c.variant != PE_KERNEL_SIMPLE && c.variant != PE_KERNEL_COLUMN)
-        return fail(PE_ERR_INVALID, "variant must be PE_KERNEL_TILED, PE_KERNEL_SIMPLE or PE_KERNEL_COLUMN");
+    if (c.variant != PE_KERNEL_TILED && c.variant != PE_KERNEL_SIMPLE && c.variant != PE_KERNEL_COLUMN &&
+        c.variant != PE_KERNEL_DENSE)
+        return fail(PE_ERR_INVALID, "variant must be PE_KERNEL_TILED, PE_KERNEL_SIMPLE, PE_KERNEL_COLUMN "
+                                    "or PE_KERNEL_DENSE");
     S->variant = c.variant;
     if (c.tile_x > 0 && c.tile_y > 0) {
         const TileShape ok[] = {{32, 8}, {32, 4}};
         bool found = false;
         for (auto t : ok) found |= (t.tx == c.tile_x && t.ty == c.tile_y);
-        if (!found || S->variant != PE_KERNEL_SIMPLE)
+        if (!found || (S->variant != PE_KERNEL_SIMPLE && S->variant != PE_KERNEL_DENSE))
             return fail(PE_ERR_UNSUPPORTED, "tile shape not compiled in for this kernel variant");
         S->tx = c.tile_x;
         S->ty = c.tile_y;
@@ -600,12 +607,15 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     if ((rc = dev_alloc(&S->status, sizeof(int)))) return rc;
     PE_CUDA(cudaMemsetAsync(S->status, 0, sizeof(int), st));
 
-    // labels: copy + range check, then mark source / receiver cells
+    // labels: copy + range check, then mark source / receiver cells (per-cell
+    // media: no material bits, only the flags)
+    if (dense) PE_CUDA(cudaMemsetAsync(S->lab, 0, sizeof(uint16_t) * ncell, st));
     unsigned long long *nbad = nullptr;
     if ((rc = dev_alloc(&nbad, sizeof(unsigned long long)))) return rc;
     PE_CUDA(cudaMemsetAsync(nbad, 0, sizeof(unsigned long long), st));
-    pe::k_labels_copy<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(md->labels_dev, S->lab, ncell,
-                                                                       c.n_mat, nbad);
+    if (!dense)
+        pe::k_labels_copy<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(md->labels_dev, S->lab, ncell,
+                                                                           c.n_mat, nbad);
     unsigned long long bad = 0;
     PE_CUDA(cudaMemcpyAsync(&bad, nbad, sizeof(bad), cudaMemcpyDeviceToHost, st));
     PE_CUDA(cudaStreamSynchronize(st));
@@ -624,7 +634,7 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
         else
             pe::k_c36_to_c21<float><<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)c36, (float *)S->c21, c.n_mat);
         PE_CUDA(cudaMemcpyAsync(S->rho, md->rho, (size_t)es * c.n_mat, cudaMemcpyHostToDevice, st));
-        if (c.dtype == PE_F32) {
+        if (c.dtype == PE_F32 && !dense) {   // the pair kernels' tables
             if ((rc = dev_alloc(&S->tab36, sizeof(float) * pe::TAB36 * c.n_mat))) return rc;
             pe::k_c21_to_tab36<<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)S->c21, S->tab36, c.n_mat);
             if ((rc = dev_alloc(&S->rinv, sizeof(float) * c.n_mat))) return rc;
@@ -829,6 +839,8 @@ extern "C" {
 int pe_solver_adjoint_step(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *residual, void *stream)
 {
     if (!S || !adj || !adj->scratch || !adj->grad) return fail(PE_ERR_INVALID, "null adjoint argument");
+    if (S->variant == PE_KERNEL_DENSE)
+        return fail(PE_ERR_UNSUPPORTED, "the adjoint runs on material tables, not per-cell media");
     for (int i = 0; i < 3; ++i)
         if (!adj->lv[i] || !adj->v_prev[i]) return fail(PE_ERR_INVALID, "adjoint velocity buffers missing");
     for (int i = 0; i < 6; ++i)
@@ -844,6 +856,8 @@ int pe_solver_adjoint_segment(PeSolver *S, const PeState *state, const PeAdjoint
 {
     if (!S || !state || !adj0 || !v_hist || !adj0->scratch || !adj0->grad)
         return fail(PE_ERR_INVALID, "null adjoint argument");
+    if (S->variant == PE_KERNEL_DENSE)
+        return fail(PE_ERR_UNSUPPORTED, "the adjoint runs on material tables, not per-cell media");
     for (int i = 0; i < 3; ++i)
         if (!adj0->lv[i] || !state->v[i]) return fail(PE_ERR_INVALID, "adjoint velocity buffers missing");
     for (int i = 0; i < 6; ++i)

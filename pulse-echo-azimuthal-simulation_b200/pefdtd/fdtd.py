@@ -376,9 +376,8 @@ def _damp_at(cells, shape, sponge, dm):
     return d
 
 
-def _compress_dense(C, rho, npdt):
-    """Per-cell stiffness dict + density -> (mats, Ct, rho_t) with one row per
-    distinct (C21, rho) combination."""
+def _media_rows(C, rho):
+    """Per-cell stiffness dict + density -> (ncell, 22) rows [C21..., rho]."""
     rho = np.asarray(rho, float)
     shape = rho.shape
     keys = [f"C{i + 1}{j + 1}" for i in range(6) for j in range(i, 6)]
@@ -387,32 +386,57 @@ def _compress_dense(C, rho, npdt):
         a = np.asarray(C.get(k, 0.0), float)
         cols.append(np.broadcast_to(a, shape).reshape(-1))
     cols.append(rho.reshape(-1))
-    M = np.stack(cols, axis=1)
-    rows, inv = np.unique(M, axis=0, return_inverse=True)
-    if len(rows) > _capi.MAX_MATERIALS:
-        raise ValueError(f"{len(rows)} distinct media exceed the {_capi.MAX_MATERIALS}-row table")
+    return np.stack(cols, axis=1), shape
+
+
+def _rows_to_tables(rows, npdt):
     C21 = rows[:, :21]
     Ct = np.zeros((len(rows), 6, 6))
     for k, (i, j) in enumerate([(i, j) for i in range(6) for j in range(i, 6)]):
         Ct[:, i, j] = C21[:, k]
         Ct[:, j, i] = C21[:, k]
-    Ct = Ct.reshape(-1, 36).astype(npdt)
-    rho_t = rows[:, 21].astype(npdt)
-    return inv.reshape(shape).astype(np.uint16), Ct, rho_t
+    return Ct.reshape(-1, 36).astype(npdt), rows[:, 21].astype(npdt)
+
+
+def _compress_dense(C, rho, npdt, media="auto"):
+    """Per-cell stiffness dict + density -> (mats, Ct, rho_t, variant).
+
+    media="table": one table row per distinct (C21, rho) combination (the
+    label kernels; at most MAX_MATERIALS rows); "dense": one row per cell
+    (the per-cell kernel variant, any medium, the reference's dense path);
+    "auto": the table when the distinct media fit it, else per cell."""
+    if media not in ("auto", "table", "dense"):
+        raise ValueError(f"media must be auto, table or dense, got {media!r}")
+    M, shape = _media_rows(C, rho)
+    if media != "dense":
+        rows, inv = np.unique(M, axis=0, return_inverse=True)
+        if len(rows) <= _capi.MAX_MATERIALS:
+            Ct, rho_t = _rows_to_tables(rows, npdt)
+            return inv.reshape(shape).astype(np.uint16), Ct, rho_t, None
+        if media == "table":
+            raise ValueError(f"{len(rows)} distinct media exceed the {_capi.MAX_MATERIALS}-row table")
+    Ct, rho_t = _rows_to_tables(M, npdt)
+    return np.zeros(shape, np.uint16), Ct, rho_t, "dense"
 
 
 def forward_fused(C, rho, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coeffs=None,
                   sponge_width=0, sponge_strength=0.09, damp_mask=None, record="pressure",
                   progress=None, *, dtype="float32", device=None, chunk_steps=0, tile=(0, 0),
-                  z_chunk=0, variant="tiled"):
+                  z_chunk=0, variant="tiled", media="auto"):
     """Dense-stiffness solve (C: dict of the 21 Voigt maps or scalars, rho:
-    (nz, ny, nx)). Distinct media are folded into a material table and run on
-    the label kernels with the dense path's end-of-step damped recording."""
+    (nz, ny, nx)), with the dense path's end-of-step damped recording.
+    Distinct media are folded into a material table and run on the label
+    kernels when they fit it (at most MAX_MATERIALS); otherwise (or with
+    media="dense") every cell keeps its own row and the per-cell kernel
+    variant runs (the reference's K1-K3 take any per-cell medium,
+    sim/core/fdtd.py:392-583)."""
     coeffs = _coeffs_or_default(coeffs, order)
     if len(coeffs) > 4:
         raise ValueError(f"order <= 8 supported ({len(coeffs)} coefficients given)")
     npdt, _ = _dtype(dtype)
-    mats, Ct, rho_t = _compress_dense(C, rho, npdt)
+    mats, Ct, rho_t, forced = _compress_dense(C, rho, npdt, media)
+    if forced is not None:
+        variant = forced
     shape = mats.shape
     sponge = sponge_axis_profiles(shape, sponge_width, sponge_strength) if sponge_width > 0 else None
     dm = np.ascontiguousarray(damp_mask, np.float32) if damp_mask is not None else None
@@ -431,7 +455,7 @@ def forward_fused(C, rho, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coef
 
 def forward(C, rho, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coeffs=None,
             sponge_width=0, sponge_strength=0.09, device="auto", record="pressure",
-            progress=None):
+            progress=None, *, media="auto"):
     """Array-path signature (:236-238). The reference computes in FP64 on the
     CPU and FP32 on a GPU; here device="cpu" selects the FP64 kernels and
     anything else FP32, both on the GPU. Repeated source cells add their
@@ -446,5 +470,5 @@ def forward(C, rho, h, dt, nt, src_pts, wavelet, rec_groups, order=8, coeffs=Non
     src = [(k, w) for k, w in merged.items()]
     out = forward_fused(C, rho, h, dt, nt, src, wavelet, rec_groups, order=order, coeffs=coeffs,
                         sponge_width=sponge_width, sponge_strength=sponge_strength,
-                        record=record, progress=progress, dtype=dtype)
+                        record=record, progress=progress, dtype=dtype, media=media)
     return out.astype(np.float64)
