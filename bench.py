@@ -540,6 +540,21 @@ def _gradients(args):
     torch.cuda.synchronize()
     t_plain = (time.perf_counter() - t0) * n / n_plain
     dev = max(float(np.abs(g - q).max() / max(np.abs(q).max(), 1e-300)) for (_, g), (_, q) in zip(many, one))
+    # chained to every grain's (theta, phi) and to the 3 fabric parameters
+    # (tilt, azimuth, log concentration about the grains' own axes)
+    t0 = time.perf_counter()
+    th_l = torch.tensor(th, requires_grad=True)
+    ph_l = torch.tensor(ph, requires_grad=True)
+    fab = torch.zeros(3, dtype=torch.float64, requires_grad=True)
+    base = torch.as_tensor(inversion.axes_of(th, ph))
+    th_f, ph_f = adjoint.theta_phi_torch(adjoint.fabric_axes(fab, base))
+    loss = 0.0
+    for az, (_, G) in zip(azs, many):
+        Gt = torch.as_tensor(np.asarray(G))
+        loss = loss + (inversion.tables21(th_l, ph_l, az) * Gt[:disk.n_grains + 1]).sum()
+        loss = loss + (inversion.tables21(th_f, ph_f, az) * Gt[:disk.n_grains + 1]).sum()
+    loss.backward()
+    t_chain = time.perf_counter() - t0
     shape = disk.base["lab"].shape
     plan = sorted({opt for w in waves for _, opt in w})
     return {"metric": "misfit + gradient solves/s, batched vs plain loop", "unit": "solves/s",
@@ -547,6 +562,8 @@ def _gradients(args):
             "angles": 2 * disk.n_grains, "plain": n / t_plain, "batched": n / t_batch,
             "speedup": t_plain / t_batch, "plain_s": t_plain, "batched_s": t_batch,
             "plain_solves_timed": n_plain, "max_rel_grad_diff": dev,
+            "angle_gradient": {"n": int(2 * disk.n_grains), "norm": float(torch.cat([th_l.grad, ph_l.grad]).norm()),
+                               "fabric_params": [float(v) for v in fab.grad], "chain_s": t_chain},
             "waves": [len(w) for w in waves], "plan_inner_offload": [list(o) for o in plan],
             "bytes_per_solve_unplanned": adjoint.adjoint_bytes(shape, K, 200),
             "device_budget_bytes": budget, "peak_allocated_bytes": int(peak),

@@ -2,6 +2,9 @@
 reference-kernel harness.
 
 * ``oracle/_build/liboracle.so``  from oracle/fdtd_oracle.c (the C restatement).
+* ``oracle/_ref/libref_gpu.so``   the same kernel strings behind
+  oracle/ref_gpu_harness.cu, compiled by nvcc for the GPU (default FMA
+  contraction, as the reference's NVRTC build).
 * ``oracle/_ref/libref_cpu.so``   from oracle/ref_harness.cpp plus the
   reference's own CUDA-C kernel strings, read from the reference module where
   it lies (``sim/core/fdtd.py`` of Jerome-Graves/pulse-echo-azimuthal-simulation)
@@ -107,8 +110,40 @@ def build_ref(force=False):
     return REF_CPU_LIB
 
 
+REF_GPU_LIB = os.path.join(REF_OUT, "libref_gpu.so")
+
+
+def build_ref_gpu(force=False):
+    """Build oracle/_ref/libref_gpu.so: the reference's kernel strings
+    (oracle/_ref/ref_kernels.inc, written by build_ref) behind the GPU driver
+    restatement oracle/ref_gpu_harness.cu, compiled by nvcc for sm_100a with
+    its default FMA contraction (as NVRTC compiles them for the reference).
+    Returns its path, or None where it cannot be built."""
+    harness = os.path.join(HERE, "ref_gpu_harness.cu")
+    inc = os.path.join(REF_OUT, "ref_kernels.inc")
+    if not os.path.exists(inc):
+        return REF_GPU_LIB if os.path.exists(REF_GPU_LIB) else None
+    if not force and _newer(REF_GPU_LIB, [inc, harness]):
+        return REF_GPU_LIB
+    nvcc = None
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc"):
+        if c and os.path.exists(c):
+            nvcc = c
+            break
+    if nvcc is None:
+        import shutil
+        nvcc = shutil.which("nvcc")
+    if nvcc is None:
+        return REF_GPU_LIB if os.path.exists(REF_GPU_LIB) else None
+    tmp = REF_GPU_LIB + ".tmp"
+    subprocess.check_call([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                           "-Xcompiler", "-fPIC", "-shared", "-I", HERE, "-o", tmp, harness])
+    os.replace(tmp, REF_GPU_LIB)
+    return REF_GPU_LIB
+
+
 def build_all(force=False):
-    return build_oracle(force), build_ref(force)
+    return build_oracle(force), build_ref(force), build_ref_gpu(force)
 
 
 if __name__ == "__main__":

@@ -1,6 +1,7 @@
 """TEST INFRASTRUCTURE ONLY — ctypes front end of the CPU oracle
-(oracle/fdtd_oracle.c) and of the reference-kernel harness
-(oracle/ref_harness.cpp, built into oracle/_ref by oracle/build.py).
+(oracle/fdtd_oracle.c) and of the reference-kernel harnesses
+(oracle/ref_harness.cpp on the host, oracle/ref_gpu_harness.cu on the GPU,
+built into oracle/_ref by oracle/build.py).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this
 module; the product package never does.
@@ -78,6 +79,102 @@ def ref_lib():
                                                 C.c_void_p, C.c_void_p, C.c_int])
         _ref = L
     return _ref
+
+
+_ref_gpu = None
+
+
+def ref_gpu_lib():
+    """The reference kernels built for the GPU (oracle/_ref/libref_gpu.so),
+    or None where they cannot be built or loaded."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        path = _build.build_ref_gpu()
+        if path is None or not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        i64p = C.c_void_p
+        L.refgpu_labels_forward.argtypes = (
+            [C.c_int] * 3 + [C.c_void_p] * 4 + [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                                C.c_float, C.c_float, C.c_int, i64p, C.c_void_p, C.c_int,
+                                                C.c_void_p, C.c_int, C.c_int, i64p, i64p, C.c_void_p,
+                                                C.c_int, C.c_void_p])
+        L.refgpu_dense_forward.argtypes = (
+            [C.c_int] * 3 + [C.c_void_p] * 7 + [C.c_int, C.c_float, C.c_float, C.c_float, i64p,
+                                                C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, i64p,
+                                                i64p, C.c_void_p, C.c_int, C.c_void_p])
+        _ref_gpu = L
+    return _ref_gpu
+
+
+def _probe_arrays(prob):
+    return (np.ascontiguousarray(prob["src_idx"], np.int64), np.ascontiguousarray(prob["src_w"], np.float32),
+            np.ascontiguousarray(prob["wavelet"], np.float32), np.ascontiguousarray(prob["rec_off"], np.int64),
+            np.ascontiguousarray(prob["rec_idx"], np.int64), np.ascontiguousarray(prob["rec_w"], np.float32))
+
+
+def run_reference_labels_gpu(prob, slab=32):
+    """The reference's own label-path kernels (strains_zp, stress_lab_u,
+    vel_zp) on the GPU, nvcc-built with default FMA contraction, launched as
+    sim/core/fdtd.py:1741-1816 launches them. Needs uint8-range materials."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise RuntimeError("GPU reference harness unavailable (oracle/_ref not built)")
+    mats = np.asarray(prob["mats"])
+    if mats.max() > 255:
+        raise ValueError("the reference label path holds materials in uint8")
+    mats = np.ascontiguousarray(mats, np.uint8)
+    nz, ny, nx = mats.shape
+    Ct = np.ascontiguousarray(prob["Ct"], np.float32).reshape(-1, 36)
+    act = np.ascontiguousarray((np.abs(Ct) > 0).any(axis=0).astype(np.int32))
+    rho = np.ascontiguousarray(prob["rho_t"], np.float32)
+    damp = prob.get("damp")
+    damp = np.ascontiguousarray(damp, np.float32) if damp is not None else None
+    coeffs = np.ascontiguousarray(prob["coeffs"], np.float32)
+    s_idx, s_w, wav, r_off, r_idx, r_w = _probe_arrays(prob)
+    nt = int(prob["nt"])
+    ng = len(r_off) - 1
+    out = np.zeros((nt, ng), np.float32)
+    rc = L.refgpu_labels_forward(nz, ny, nx, _p(mats), _p(Ct), _p(act), _p(rho), len(rho), _p(damp),
+                                 _p(coeffs), len(coeffs), float(np.float32(prob["inv_h"])),
+                                 float(np.float32(prob["dt"])), float(np.float32(prob["dt_h"])), slab,
+                                 _p(s_idx), _p(s_w), len(s_idx), _p(wav), nt, ng, _p(r_off), _p(r_idx),
+                                 _p(r_w), _REC[prob.get("record", "pressure")], _p(out))
+    if rc:
+        raise RuntimeError(f"GPU reference harness failed with code {rc}")
+    return out
+
+
+def run_reference_dense_gpu(prob):
+    """The reference's dense kernels (strains, stress_acc, vel_update) with
+    end-of-step damping on the GPU, nvcc-built with default FMA contraction,
+    launched as sim/core/fdtd.py:875-921 launches them; any number of
+    materials (36 per-cell stiffness planes)."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise RuntimeError("GPU reference harness unavailable (oracle/_ref not built)")
+    mats = np.asarray(prob["mats"]).astype(np.int64)
+    nz, ny, nx = mats.shape
+    Ct = np.asarray(prob["Ct"], np.float32).reshape(-1, 36)
+    Cflat = np.ascontiguousarray(np.moveaxis(Ct[mats], -1, 0))
+    act = np.ascontiguousarray((np.abs(Ct) > 0).any(axis=0).astype(np.int32))
+    rho_cell = np.asarray(prob["rho_t"], np.float32)[mats].astype(float)
+    rv = [np.ascontiguousarray(_face_density(rho_cell, ax), np.float32) for ax in (2, 1, 0)]
+    damp = prob.get("damp")
+    damp = np.ascontiguousarray(damp, np.float32) if damp is not None else None
+    coeffs = np.ascontiguousarray(prob["coeffs"], np.float32)
+    s_idx, s_w, wav, r_off, r_idx, r_w = _probe_arrays(prob)
+    nt = int(prob["nt"])
+    ng = len(r_off) - 1
+    out = np.zeros((nt, ng), np.float32)
+    rc = L.refgpu_dense_forward(nz, ny, nx, _p(Cflat), _p(act), _p(rv[0]), _p(rv[1]), _p(rv[2]), _p(damp),
+                                _p(coeffs), len(coeffs), float(np.float32(prob["inv_h"])),
+                                float(np.float32(prob["dt"])), float(np.float32(prob["dt_h"])), _p(s_idx),
+                                _p(s_w), len(s_idx), _p(wav), nt, ng, _p(r_off), _p(r_idx), _p(r_w),
+                                _REC[prob.get("record", "pressure")], _p(out))
+    if rc:
+        raise RuntimeError(f"GPU reference harness failed with code {rc}")
+    return out
 
 
 def run_oracle(prob, dtype=np.float32, fma_mode=1, n_threads=0, return_state=False):

@@ -67,8 +67,10 @@ __device__ __forceinline__ float adj_damp(const AdjArgs<T> &A, int iz, int iy, i
 }
 
 // transpose of the forward derivative along one axis, at position y of an
-// axis of length n; f(o) reads the operand at y + o (only called where the
-// forward cell y + o exists)
+// axis of length n; f(o) reads the operand at y + o. A tap whose forward cell
+// y + o does not exist reads the operand at y instead (always in the grid)
+// and contributes c * 0, which leaves the sum unchanged bit for bit: every
+// load is independent of the guards, so the gathers of a cell overlap.
 template <typename T, typename F>
 __device__ __forceinline__ T DfT(const F &f, int y, int n, const T c[4], int nc)
 {
@@ -76,8 +78,10 @@ __device__ __forceinline__ T DfT(const F &f, int y, int n, const T c[4], int nc)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (j < nc) {
-            if (gF(y - j - 1, j, n)) a += c[j] * f(-j - 1);
-            if (gF(y + j, j, n)) a -= c[j] * f(j);
+            const bool p1 = gF(y - j - 1, j, n), p2 = gF(y + j, j, n);
+            const T v1 = f(p1 ? -j - 1 : 0), v2 = f(p2 ? j : 0);
+            a += c[j] * (p1 ? v1 : T(0));
+            a -= c[j] * (p2 ? v2 : T(0));
         }
     }
     return a;
@@ -89,8 +93,10 @@ __device__ __forceinline__ T DbT(const F &f, int y, int n, const T c[4], int nc)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (j < nc) {
-            if (gB(y - j, j, n)) a += c[j] * f(-j);
-            if (gB(y + j + 1, j, n)) a -= c[j] * f(j + 1);
+            const bool p1 = gB(y - j, j, n), p2 = gB(y + j + 1, j, n);
+            const T v1 = f(p1 ? -j : 0), v2 = f(p2 ? j + 1 : 0);
+            a += c[j] * (p1 ? v1 : T(0));
+            a -= c[j] * (p2 ? v2 : T(0));
         }
     }
     return a;
@@ -102,6 +108,21 @@ __device__ __forceinline__ void cell_of(const AdjArgs<T> &A, long long i, int &i
     ix = (int)(i % A.nx);
     iy = (int)((i / A.nx) % A.ny);
     iz = (int)(i / ((long long)A.nx * A.ny));
+}
+
+// Cell of this thread in the adjoint kernels' launches: 32 x 8 blocks over
+// (x tiles, y tiles, z planes), so that a warp is 32 consecutive cells of a
+// row and the coordinates come from the launch indices (no 64-bit division
+// per cell). False for the threads past the grid's x / y edge.
+constexpr int ADJ_BX = 32, ADJ_BY = 8;
+template <typename T>
+__device__ __forceinline__ bool adj_cell(const AdjArgs<T> &A, long long &i, int &iz, int &iy, int &ix)
+{
+    ix = blockIdx.x * ADJ_BX + threadIdx.x;
+    iy = blockIdx.y * ADJ_BY + threadIdx.y;
+    iz = blockIdx.z;
+    i = ((long long)iz * A.ny + iy) * A.nx + ix;
+    return ix < A.nx && iy < A.ny;
 }
 
 // ---------------------------------------------------------------- receivers
@@ -148,10 +169,9 @@ __device__ __forceinline__ float adj_div<float>(float a, float b, float r0, cons
 template <typename T>
 __global__ void k_adj_vel_u(AdjArgs<T> A)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    long long i;
     int iz, iy, ix;
-    cell_of(A, i, iz, iy, ix);
+    if (!adj_cell(A, i, iz, iy, ix)) return;
     const int m0 = A.lab[i] & LAB_MAT;
     const T r0 = A.rho[m0];
     const T rvx = ix < A.nx - 1 ? T(0.5) * (r0 + A.rho[A.lab[i + 1] & LAB_MAT]) : r0;
@@ -166,10 +186,9 @@ __global__ void k_adj_vel_u(AdjArgs<T> A)
 template <typename T>
 __global__ void k_adj_vel(AdjArgs<T> A)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    long long i;
     int iz, iy, ix;
-    cell_of(A, i, iz, iy, ix);
+    if (!adj_cell(A, i, iz, iy, ix)) return;
     const long long sy = A.sy, sz = A.sz;
     const T *ux = A.u[0] + i, *uy = A.u[1] + i, *uz = A.u[2] + i;
     auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
@@ -187,26 +206,32 @@ __global__ void k_adj_vel(AdjArgs<T> A)
 template <typename T>
 __global__ void k_adj_strain(AdjArgs<T> A)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    long long i;
     int iz, iy, ix;
-    cell_of(A, i, iz, iy, ix);
+    if (!adj_cell(A, i, iz, iy, ix)) return;
     const long long sy = A.sy, sz = A.sz;
     const T *vx = A.vp[0], *vy = A.vp[1], *vz = A.vp[2];
     T a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
+    // a skipped tap reads the cell itself twice: its difference is +0 and
+    // fmac(a, c, +0) == a bit for bit, so the loads need not wait on guards
+    auto d = [&](const T *f, bool ok, long long hi, long long lo) -> T {
+        return f[ok ? i + hi : i] - f[ok ? i + lo : i];
+    };
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (j < A.nc) {
             const T cj = A.c[j];
-            if (gB(ix, j, A.nx)) a1 = fmac(a1, cj, vx[i + j] - vx[i - (j + 1)]);
-            if (gB(iy, j, A.ny)) a2 = fmac(a2, cj, vy[i + j * sy] - vy[i - (j + 1) * sy]);
-            if (gB(iz, j, A.nz)) a3 = fmac(a3, cj, vz[i + j * sz] - vz[i - (j + 1) * sz]);
-            if (gF(iy, j, A.ny)) a4 = fmac(a4, cj, vz[i + (j + 1) * sy] - vz[i - j * sy]);
-            if (gF(iz, j, A.nz)) a4 = fmac(a4, cj, vy[i + (j + 1) * sz] - vy[i - j * sz]);
-            if (gF(ix, j, A.nx)) a5 = fmac(a5, cj, vz[i + (j + 1)] - vz[i - j]);
-            if (gF(iz, j, A.nz)) a5 = fmac(a5, cj, vx[i + (j + 1) * sz] - vx[i - j * sz]);
-            if (gF(ix, j, A.nx)) a6 = fmac(a6, cj, vy[i + (j + 1)] - vy[i - j]);
-            if (gF(iy, j, A.ny)) a6 = fmac(a6, cj, vx[i + (j + 1) * sy] - vx[i - j * sy]);
+            const bool bx = gB(ix, j, A.nx), by = gB(iy, j, A.ny), bz = gB(iz, j, A.nz);
+            const bool fx = gF(ix, j, A.nx), fy = gF(iy, j, A.ny), fz = gF(iz, j, A.nz);
+            a1 = fmac(a1, cj, d(vx, bx, j, -(j + 1)));
+            a2 = fmac(a2, cj, d(vy, by, j * sy, -(j + 1) * sy));
+            a3 = fmac(a3, cj, d(vz, bz, j * sz, -(j + 1) * sz));
+            a4 = fmac(a4, cj, d(vz, fy, (j + 1) * sy, -j * sy));
+            a4 = fmac(a4, cj, d(vy, fz, (j + 1) * sz, -j * sz));
+            a5 = fmac(a5, cj, d(vz, fx, j + 1, -j));
+            a5 = fmac(a5, cj, d(vx, fz, (j + 1) * sz, -j * sz));
+            a6 = fmac(a6, cj, d(vy, fx, j + 1, -j));
+            a6 = fmac(a6, cj, d(vx, fy, (j + 1) * sy, -j * sy));
         }
     }
     const T ih = A.inv_h;
@@ -241,8 +266,9 @@ __host__ __device__ constexpr int adj_widx(int J, int p)
 template <typename T>
 __global__ void k_adj_w(AdjArgs<T> A)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    long long i;
+    int iz, iy, ix;
+    if (!adj_cell(A, i, iz, iy, ix)) return;
     const int VP[6] = {0, 0, 0, 1, 2, 3};
     const T *Cx = A.c21 + (long long)(A.lab[i] & LAB_MAT) * C21_STRIDE;
     T e[6];
@@ -261,50 +287,120 @@ __global__ void k_adj_w(AdjArgs<T> A)
         }
 }
 
-constexpr int ADJ_STRESS_WARPS = 8;   // k_adj_stress runs 256-thread blocks
+constexpr int ADJ_STRESS_WARPS = ADJ_BY;   // k_adj_stress blocks: one warp per row of the 32 x 8 tile
+static_assert(ADJ_BX == 32, "a warp is one row of an adjoint block");
+
+// strain J moved to position P at cell i (the forward's half-cell move,
+// same tap order). The taps are loaded unconditionally, from the cell itself
+// where the move is off the grid, and masked afterwards: no load waits on a
+// guard, so the gathers of a cell are all in flight together.
+template <typename T, int P, int J>
+__device__ __forceinline__ T adj_q(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
+{
+    constexpr int S = vpos(J);
+    constexpr int DZ = pos_z(P) - pos_z(S), DY = pos_y(P) - pos_y(S), DX = pos_x(P) - pos_x(S);
+    if constexpr (DZ == 0 && DY == 0 && DX == 0) {
+        return A.g[J][i];
+    } else {
+        const bool ok = move_ok(iz, iy, ix, DZ, DY, DX, A.nz, A.ny, A.nx);
+        const T *g = A.g[J];
+        T acc = 0;
+#pragma unroll
+        for (int a0 = (DZ < 0 ? -1 : 0); a0 <= (DZ > 0 ? 1 : 0); ++a0)
+#pragma unroll
+            for (int a1 = (DY < 0 ? -1 : 0); a1 <= (DY > 0 ? 1 : 0); ++a1)
+#pragma unroll
+                for (int a2 = (DX < 0 ? -1 : 0); a2 <= (DX > 0 ? 1 : 0); ++a2)
+                    acc += g[ok ? i + a0 * A.sz + a1 * A.sy + a2 : i];
+        return ok ? acc * T(0.25) : T(0);
+    }
+}
+
+// strain adjoint t_J, the contribution of position P: the direct term (P the
+// position of J) or the transposed move of W[P][J] gathered from the forward
+// cells x = i - o of every tap offset o (guards evaluated at x, loads
+// unconditional as in adj_q)
+template <typename T, int J, int P>
+__device__ __forceinline__ void adj_t(const AdjArgs<T> &A, long long i, int iz, int iy, int ix, const T *Cm,
+                                      const T (&e)[6], T &acc)
+{
+    constexpr int S = vpos(J);
+    constexpr int DZ = pos_z(P) - pos_z(S), DY = pos_y(P) - pos_y(S), DX = pos_x(P) - pos_x(S);
+    if constexpr (DZ == 0 && DY == 0 && DX == 0) {
+#pragma unroll
+        for (int I = 0; I < 6; ++I)
+            if (vpos(I) == P) acc += Cm[c21_slot(I, J)] * e[I];
+    } else {
+        const T *w = A.w[adj_widx(J, P)];
+#pragma unroll
+        for (int a0 = (DZ < 0 ? -1 : 0); a0 <= (DZ > 0 ? 1 : 0); ++a0)
+#pragma unroll
+            for (int a1 = (DY < 0 ? -1 : 0); a1 <= (DY > 0 ? 1 : 0); ++a1)
+#pragma unroll
+                for (int a2 = (DX < 0 ? -1 : 0); a2 <= (DX > 0 ? 1 : 0); ++a2) {
+                    const bool ok = move_ok(iz - a0, iy - a1, ix - a2, DZ, DY, DX, A.nz, A.ny, A.nx);
+                    const T v = w[ok ? i - a0 * A.sz - a1 * A.sy - a2 : i];
+                    acc += T(0.25) * (ok ? v : T(0));
+                }
+    }
+}
+
+template <typename T, int J>
+__device__ __forceinline__ T adj_tJ(const AdjArgs<T> &A, long long i, int iz, int iy, int ix, const T *Cm,
+                                    const T (&e)[6])
+{
+    T acc = 0;
+    adj_t<T, J, 0>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 1>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 2>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 3>(A, i, iz, iy, ix, Cm, e, acc);
+    return acc;
+}
+
+template <typename T, int P>
+__device__ __forceinline__ void adj_qrow(const AdjArgs<T> &A, long long i, int iz, int iy, int ix, T (&q)[6])
+{
+    q[0] = adj_q<T, P, 0>(A, i, iz, iy, ix);
+    q[1] = adj_q<T, P, 1>(A, i, iz, iy, ix);
+    q[2] = adj_q<T, P, 2>(A, i, iz, iy, ix);
+    q[3] = adj_q<T, P, 3>(A, i, iz, iy, ix);
+    q[4] = adj_q<T, P, 4>(A, i, iz, iy, ix);
+    q[5] = adj_q<T, P, 5>(A, i, iz, iy, ix);
+}
 
 template <typename T>
 __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T> A)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < (long long)A.nz * A.ny * A.nx;
-    int iz = 0, iy = 0, ix = 0;
-    if (live) cell_of(A, i, iz, iy, ix);
-    const int nz = A.nz, ny = A.ny, nx = A.nx;
-    const long long sy = A.sy, sz = A.sz;
-    const int POSZ[4] = {0, 1, 1, 0}, POSY[4] = {0, 1, 0, 1}, POSX[4] = {0, 0, 1, 1};
-    const int VP[6] = {0, 0, 0, 1, 2, 3};
-    double gsum[21];
-#pragma unroll
-    for (int k = 0; k < 21; ++k) gsum[k] = 0.0;
-    int m = 0;
+    long long i;
+    int iz, iy, ix;
+    const bool live = adj_cell(A, i, iz, iy, ix);
+    // Per-material gradient, summed per warp: every lane writes its 21 terms
+    // to its row of the warp's 32 x 21 tile in shared memory (zero where the
+    // cell is off the grid), then for each distinct material of the warp
+    // lanes 0..20 each add up one column over the lanes of that material and
+    // issue the 21 f64 atomics together. Writing the terms out as they are
+    // formed keeps them out of registers during the gathers that follow.
+    // Warps add into one of grad_rep replicas of the table (by warp index),
+    // so that the warps of a large single-material region (the couplant) do
+    // not all serialise on the same 21 addresses. Tile rows are 21 doubles
+    // apart: row stores and column loads are free of bank conflicts.
+    __shared__ double red[ADJ_STRESS_WARPS][32][21];
+    __shared__ int rmat[ADJ_STRESS_WARPS][32];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.y;
+    int m = -1;
+    bool any = false;
+    T e[6];
     if (live) {
         m = A.lab[i] & LAB_MAT;
-        const T *Cm = A.c21 + (long long)m * C21_STRIDE;
-        T e[6];
 #pragma unroll
         for (int I = 0; I < 6; ++I) e[I] = A.dt * A.ls[I][i];
         // moved strains at this cell, q[p][J]
         T q[4][6];
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int J = 0; J < 6; ++J) {
-                const int s = VP[J];
-                const int dz = POSZ[p] - POSZ[s], dy = POSY[p] - POSY[s], dx = POSX[p] - POSX[s];
-                if (dz == 0 && dy == 0 && dx == 0) {
-                    q[p][J] = A.g[J][i];
-                } else if (!move_ok(iz, iy, ix, dz, dy, dx, nz, ny, nx)) {
-                    q[p][J] = 0;
-                } else {
-                    T acc = 0;
-                    for (int a0 = (dz < 0 ? -1 : 0); a0 <= (dz > 0 ? 1 : 0); ++a0)
-                        for (int a1 = (dy < 0 ? -1 : 0); a1 <= (dy > 0 ? 1 : 0); ++a1)
-                            for (int a2 = (dx < 0 ? -1 : 0); a2 <= (dx > 0 ? 1 : 0); ++a2)
-                                acc += A.g[J][i + a0 * sz + a1 * sy + a2];
-                    q[p][J] = acc * T(0.25);
-                }
-            }
+        adj_qrow<T, 0>(A, i, iz, iy, ix, q[0]);
+        adj_qrow<T, 1>(A, i, iz, iy, ix, q[1]);
+        adj_qrow<T, 2>(A, i, iz, iy, ix, q[2]);
+        adj_qrow<T, 3>(A, i, iz, iy, ix, q[3]);
         // dJ/dC_IJ for I <= J: e_I q[p(I)][J] + e_J q[p(J)][I]  (I != J),
         // formed in the solve's precision (in FP32 one rounding of the
         // cell's term, as its fields carry) and summed over cells in f64
@@ -312,86 +408,57 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
         for (int I = 0; I < 6; ++I)
 #pragma unroll
             for (int J = I; J < 6; ++J) {
-                T v = e[I] * q[VP[I]][J];
-                if (J != I) v += e[J] * q[VP[J]][I];
-                gsum[c21_slot(I, J)] = (double)v;
+                T v = e[I] * q[vpos(I)][J];
+                if (J != I) v += e[J] * q[vpos(J)][I];
+                red[warp][lane][c21_slot(I, J)] = (double)v;
+                any = any || v != T(0);
             }
-        // strain adjoint t_J: direct term plus transposed moves of
-        // W[p][J](x) = sum_{I at p} C_IJ(x) e_I(x) from the forward cells x
-        T tJ[6];
+    } else {
 #pragma unroll
-        for (int J = 0; J < 6; ++J) {
-            const int s = VP[J];
-            T acc = 0;
-            for (int p = 0; p < 4; ++p) {
-                const int dz = POSZ[p] - POSZ[s], dy = POSY[p] - POSY[s], dx = POSX[p] - POSX[s];
-                if (dz == 0 && dy == 0 && dx == 0) {
-                    for (int I = 0; I < 6; ++I)
-                        if (VP[I] == p) acc += Cm[c21_slot(I, J)] * e[I];
-                    continue;
-                }
-                // forward cells x = y - o for every tap offset o of this move
-                for (int a0 = (dz < 0 ? -1 : 0); a0 <= (dz > 0 ? 1 : 0); ++a0)
-                    for (int a1 = (dy < 0 ? -1 : 0); a1 <= (dy > 0 ? 1 : 0); ++a1)
-                        for (int a2 = (dx < 0 ? -1 : 0); a2 <= (dx > 0 ? 1 : 0); ++a2) {
-                            const int xz = iz - a0, xy = iy - a1, xx = ix - a2;
-                            if (!move_ok(xz, xy, xx, dz, dy, dx, nz, ny, nx)) continue;
-                            const long long xi = i - a0 * sz - a1 * sy - a2;
-                            acc += T(0.25) * A.w[adj_widx(J, p)][xi];
-                        }
-            }
-            tJ[J] = acc;
-        }
-#pragma unroll
-        for (int J = 0; J < 6; ++J) A.t[J][i] = tJ[J];
-        // the step's last use of ls at this cell (k_adj_w ran before, and
-        // only this thread reads it here): apply the deferred damping,
-        // ls = d ls (the transpose of the forward s^{n-1} * d)
-        const T d = (T)adj_damp(A, iz, iy, ix, i);
-#pragma unroll
-        for (int I = 0; I < 6; ++I) A.ls[I][i] = d * A.ls[I][i];
+        for (int k = 0; k < 21; ++k) red[warp][lane][k] = 0.0;
     }
-    // per-material gradient, once per distinct material in the warp: every
-    // lane writes its 21 sums (zero for other materials) to the warp's
-    // 32 x 21 tile in shared memory, then lanes 0..20 each add up one column
-    // and issue the 21 f64 atomics together. Warps add into one of grad_rep
-    // replicas of the table (by warp index), so that the warps of a large
-    // single-material region (the couplant) do not all serialise on the same
-    // 21 addresses. Tile rows are 21 doubles apart: the row stores and the
-    // column loads are both free of bank conflicts.
-    __shared__ double red[ADJ_STRESS_WARPS][32][21];
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    rmat[warp][lane] = m;
+    __syncwarp();
     double *gtab = A.grad;
     if (A.grad_rep > 1)
-        gtab += (long long)((blockIdx.x * (blockDim.x >> 5) + warp) % (unsigned)A.grad_rep) * A.n_mat * 21;
+        gtab += (long long)(((blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x * ADJ_BY + blockIdx.x * ADJ_BY + warp) %
+                            (unsigned)A.grad_rep) * A.n_mat * 21;
     // lanes whose 21 terms are all zero (no overlap of the adjoint stress
     // and the forward strain at the cell) add nothing and sit out
-    bool any = false;
-#pragma unroll
-    for (int k = 0; k < 21; ++k) any = any || gsum[k] != 0.0;
-    const int my = live ? m : -1;
     unsigned remaining = __ballot_sync(full, live && any);
+    const int my = live && any ? m : -1;
     while (remaining) {
         const int src = __ffs(remaining) - 1;
         const int mm = __shfl_sync(full, my, src);
         remaining &= ~__ballot_sync(full, my == mm);
-#pragma unroll
-        for (int k = 0; k < 21; ++k) red[warp][lane][k] = my == mm ? gsum[k] : 0.0;
-        __syncwarp();
         if (lane < 21) {
             double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;   // four chains, for latency
 #pragma unroll
             for (int r = 0; r < 32; r += 4) {
-                v0 += red[warp][r][lane];
-                v1 += red[warp][r + 1][lane];
-                v2 += red[warp][r + 2][lane];
-                v3 += red[warp][r + 3][lane];
+                v0 += rmat[warp][r] == mm ? red[warp][r][lane] : 0.0;
+                v1 += rmat[warp][r + 1] == mm ? red[warp][r + 1][lane] : 0.0;
+                v2 += rmat[warp][r + 2] == mm ? red[warp][r + 2][lane] : 0.0;
+                v3 += rmat[warp][r + 3] == mm ? red[warp][r + 3][lane] : 0.0;
             }
             atomicAdd(gtab + (long long)mm * 21 + lane, (v0 + v1) + (v2 + v3));
         }
-        __syncwarp();
     }
+    if (!live) return;
+    // strain adjoint t_J: direct term plus transposed moves of
+    // W[p][J](x) = sum_{I at p} C_IJ(x) e_I(x) from the forward cells x
+    const T *Cm = A.c21 + (long long)m * C21_STRIDE;
+    A.t[0][i] = adj_tJ<T, 0>(A, i, iz, iy, ix, Cm, e);
+    A.t[1][i] = adj_tJ<T, 1>(A, i, iz, iy, ix, Cm, e);
+    A.t[2][i] = adj_tJ<T, 2>(A, i, iz, iy, ix, Cm, e);
+    A.t[3][i] = adj_tJ<T, 3>(A, i, iz, iy, ix, Cm, e);
+    A.t[4][i] = adj_tJ<T, 4>(A, i, iz, iy, ix, Cm, e);
+    A.t[5][i] = adj_tJ<T, 5>(A, i, iz, iy, ix, Cm, e);
+    // the step's last use of ls at this cell (k_adj_w ran before, and only
+    // this thread reads it here): apply the deferred damping, ls = d ls (the
+    // transpose of the forward s^{n-1} * d)
+    const T d = (T)adj_damp(A, iz, iy, ix, i);
+#pragma unroll
+    for (int I = 0; I < 6; ++I) A.ls[I][i] = d * A.ls[I][i];
 }
 
 // grad += sum of the replicas, which are left zero
@@ -410,10 +477,9 @@ __global__ void k_grad_fold(double *rep, int nrep, long long len, double *grad)
 template <typename T>
 __global__ void k_adj_velfin(AdjArgs<T> A)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)A.nz * A.ny * A.nx) return;
+    long long i;
     int iz, iy, ix;
-    cell_of(A, i, iz, iy, ix);
+    if (!adj_cell(A, i, iz, iy, ix)) return;
     const long long sy = A.sy, sz = A.sz;
     auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
     auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };

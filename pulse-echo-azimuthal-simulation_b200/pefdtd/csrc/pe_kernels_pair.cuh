@@ -209,18 +209,18 @@ __device__ __forceinline__ void pair_strain(const StepArgs<float> &A, int q, con
             const float2 yp = lds2(tvy + j * W), ym = lds2(tvy - (j + 1) * W);     // Dby vy
             const float2 zp = lds2(tvz + (j + 1) * W), zm = lds2(tvz - j * W);     // Dfy vz
             const float2 xp = lds2(tvx + (j + 1) * W), xm = lds2(tvx - j * W);     // Dfy vx
-            // per lane: a1 x; a2 y; a3 z; a4 y, z; a5 x, z; a6 x, y
-            a1.x = fmac(a1.x, cxb0, X[4 + j] - X[3 - j]);
-            a1.y = fmac(a1.y, cxb1, X[5 + j] - X[4 - j]);
+            // per lane: a1 x; a2 y; a3 z; a4 y, z; a5 x, z; a6 x, y. The x
+            // taps' differences are per lane (their operands straddle the
+            // lanes' 64-bit pairs), their fused multiply-adds paired
+            const float2 cxb = make_float2(cxb0, cxb1), cxf = make_float2(cxf0, cxf1);
+            a1 = fmac2(a1, cxb, make_float2(X[4 + j] - X[3 - j], X[5 + j] - X[4 - j]));
             a2 = fmac2(a2, bc2(cyb), sub2(yp, ym));
             a3 = fmac2(a3, bc2(czb), sub2(rz[4 + j], rz[3 - j]));
             a4 = fmac2(a4, bc2(cyf), sub2(zp, zm));
             a4 = fmac2(a4, bc2(czf), sub2(ry[4 + j], ry[3 - j]));
-            a5.x = fmac(a5.x, cxf0, Z[5 + j] - Z[4 - j]);
-            a5.y = fmac(a5.y, cxf1, Z[6 + j] - Z[5 - j]);
+            a5 = fmac2(a5, cxf, make_float2(Z[5 + j] - Z[4 - j], Z[6 + j] - Z[5 - j]));
             a5 = fmac2(a5, bc2(czf), sub2(rx[4 + j], rx[3 - j]));
-            a6.x = fmac(a6.x, cxf0, Y[5 + j] - Y[4 - j]);
-            a6.y = fmac(a6.y, cxf1, Y[6 + j] - Y[5 - j]);
+            a6 = fmac2(a6, cxf, make_float2(Y[5 + j] - Y[4 - j], Y[6 + j] - Y[5 - j]));
             a6 = fmac2(a6, bc2(cyf), sub2(xp, xm));
         }
     }
@@ -804,13 +804,12 @@ __device__ __forceinline__ void pair_vel_taps(const StepArgs<float> &A, int z, c
             const float cyf = tapc<G>(cj, j, tl.yf), cyb = tapc<G>(cj, j, tl.yb);
             const float cxb0 = tapc<G>(cj, j, tl.xb[0]), cxb1 = tapc<G>(cj, j, tl.xb[1]);
             const float cxf0 = tapc<G>(cj, j, tl.xf[0]), cxf1 = tapc<G>(cj, j, tl.xf[1]);
-            // per lane: x taps, then y, then z, for each of ax, ay, az
-            ax.x = fmac(ax.x, cxf0, S1[5 + j] - S1[4 - j]);
-            ax.y = fmac(ax.y, cxf1, S1[6 + j] - S1[5 - j]);
-            ay.x = fmac(ay.x, cxb0, S6[4 + j] - S6[3 - j]);
-            ay.y = fmac(ay.y, cxb1, S6[5 + j] - S6[4 - j]);
-            az.x = fmac(az.x, cxb0, S5[4 + j] - S5[3 - j]);
-            az.y = fmac(az.y, cxb1, S5[5 + j] - S5[4 - j]);
+            // per lane: x taps, then y, then z, for each of ax, ay, az (x-tap
+            // differences per lane, their fused multiply-adds paired)
+            const float2 cxb = make_float2(cxb0, cxb1), cxf = make_float2(cxf0, cxf1);
+            ax = fmac2(ax, cxf, make_float2(S1[5 + j] - S1[4 - j], S1[6 + j] - S1[5 - j]));
+            ay = fmac2(ay, cxb, make_float2(S6[4 + j] - S6[3 - j], S6[5 + j] - S6[4 - j]));
+            az = fmac2(az, cxb, make_float2(S5[4 + j] - S5[3 - j], S5[5 + j] - S5[4 - j]));
             ay = fmac2(ay, bc2(cyf), sub2(p2, m2));
             ax = fmac2(ax, bc2(cyb), sub2(p6, m6));
             az = fmac2(az, bc2(cyb), sub2(p4, m4));

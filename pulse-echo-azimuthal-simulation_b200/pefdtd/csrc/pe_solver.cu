@@ -815,19 +815,23 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
     A.grad = grad;
     A.grad_rep = nrep;
     A.n_mat = c.n_mat;
-    const unsigned nb = (unsigned)((ncell + 255) / 256);
+    if (c.nz > 65535) return fail(PE_ERR_UNSUPPORTED, "the adjoint launches one block row per z plane (nz <= 65535)");
     if (S->n_rec > 0 && residual) {
         const T *row = (const T *)residual + (size_t)n * S->n_groups;
         pe::k_adj_inject<T><<<(S->n_rec + 127) / 128, 128, 0, st>>>(A, S->rec_cell, S->rec_pos, (const T *)S->rec_w,
                                                                      S->ent_group, S->n_rec, row, c.record,
                                                                      c.damped_record);
     }
-    pe::k_adj_vel_u<T><<<nb, 256, 0, st>>>(A);
-    pe::k_adj_vel<T><<<nb, 256, 0, st>>>(A);
-    pe::k_adj_strain<T><<<nb, 256, 0, st>>>(A);
-    pe::k_adj_w<T><<<nb, 256, 0, st>>>(A);
-    pe::k_adj_stress<T><<<nb, 256, 0, st>>>(A);
-    pe::k_adj_velfin<T><<<nb, 256, 0, st>>>(A);
+    // cell kernels: 32 x 8 blocks over (x tiles, y tiles, z planes)
+    const dim3 ab(pe::ADJ_BX, pe::ADJ_BY, 1);
+    const dim3 ag((unsigned)((c.nx + pe::ADJ_BX - 1) / pe::ADJ_BX), (unsigned)((c.ny + pe::ADJ_BY - 1) / pe::ADJ_BY),
+                  (unsigned)c.nz);
+    pe::k_adj_vel_u<T><<<ag, ab, 0, st>>>(A);
+    pe::k_adj_vel<T><<<ag, ab, 0, st>>>(A);
+    pe::k_adj_strain<T><<<ag, ab, 0, st>>>(A);
+    pe::k_adj_w<T><<<ag, ab, 0, st>>>(A);
+    pe::k_adj_stress<T><<<ag, ab, 0, st>>>(A);
+    pe::k_adj_velfin<T><<<ag, ab, 0, st>>>(A);
     PE_CUDA(cudaGetLastError());
     return PE_OK;
 }

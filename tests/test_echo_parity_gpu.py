@@ -18,6 +18,13 @@ same kernels stated.
 * disk_prod (160 x 256 x 256, 500 grains) over the first 1800 steps (burst
   and bottom echo) against the reference's dense kernels, whose trace is a
   fixture (tests/golden/make_disk_prod_echo.py; tens of minutes on the host).
+
+The "reference's own update" is checked in both of its builds: the host
+build (oracle/_ref/libref_cpu.so, every product rounded separately) and the
+GPU build (oracle/_ref/libref_gpu.so: the reference's kernel strings compiled
+by nvcc with default FMA contraction, as its NVRTC build runs them, launched
+with its launch shapes). The GPU build makes the full 6000 steps of disk_prod
+affordable, so that configuration is compared over its whole length.
 """
 import os
 
@@ -101,5 +108,62 @@ def test_disk_prod_first_1800_steps_vs_reference_dense_fixture():
     (pa, pb, pc), t_lo, w_lo, w_hi = _echo_picks(p, tr, ref, tr64)
     for q in (pa, pb, pc):
         assert q[2] and w_lo <= q[0] <= w_hi
+    assert round(pa[0] / p["dt"]) == round(pb[0] / p["dt"]) == round(pc[0] / p["dt"])
+    assert abs(pa[0] - pb[0]) < 1e-3 * p["dt"]
+
+
+def _need_gpu_ref():
+    if O.ref_gpu_lib() is None:
+        pytest.skip("GPU reference harness not built")
+
+
+def test_gpu_reference_harness_agrees_with_host_build():
+    """The two builds of the reference's kernels differ only by FMA
+    contraction."""
+    from helpers import make_small
+    _need_gpu_ref()
+    if O.ref_lib() is None:
+        pytest.skip("reference harness not built")
+    p = make_small(nt=200, shape=(24, 30, 32), n_grains=9, sponge=4)
+    for record in ("pressure", "vz"):
+        pr = oracle_prob(p, record=record, damped_record=False)
+        a, b = O.run_reference_labels_gpu(pr), O.run_reference_labels(pr)
+        assert np.abs(b).max() > 0 and rel_l2(a, b) < 1e-5
+        prd = oracle_prob(p, record=record, damped_record=True)
+        a, b = O.run_reference_dense_gpu(prd), O.run_reference_dense(prd)
+        assert rel_l2(a, b) < 1e-5
+
+
+def test_disk_small_echo_variant_vs_gpu_reference():
+    from pefdtd import workloads
+    _need_gpu_ref()
+    p = workloads.make_problem(dict(workloads.WORKLOADS["disk_small"], sponge=6))
+    tr = _fwd(p)
+    pr = oracle_prob(p, record="vz", damped_record=True)
+    ref = O.run_reference_labels_gpu(pr)
+    assert rel_l2(tr, ref) < TOL
+    (pa, pb), t_lo, w_lo, w_hi = _echo_picks(p, tr, ref)
+    assert pa[2] and pb[2] and w_lo <= pa[0] <= w_hi
+    assert round(pa[0] / p["dt"]) == round(pb[0] / p["dt"])
+    assert abs(pa[0] - pb[0]) < 1e-3 * p["dt"]
+
+
+def test_disk_prod_full_length_vs_gpu_reference_dense():
+    """disk_prod over its full 6000 steps against the reference's dense
+    kernels on the GPU (500 grains: beyond the uint8 label path), the bottom
+    echo picked identically, and the FP64 run of the same kernels."""
+    from pefdtd import workloads
+    _need_gpu_ref()
+    p = workloads.make_problem("disk_prod")
+    assert p["nt"] == 6000
+    tr = _fwd(p)
+    ref = O.run_reference_dense_gpu(oracle_prob(p, record="vz", damped_record=True))
+    tr64 = _fwd(p, dtype="float64")
+    assert rel_l2(tr, ref) < TOL
+    assert rel_l2(tr, tr64) < TOL
+    (pa, pb, pc), t_lo, w_lo, w_hi = _echo_picks(p, tr, ref, tr64)
+    for q in (pa, pb, pc):
+        assert q[2] and w_lo <= q[0] <= w_hi
+    assert pa[1] > 0.3 * np.abs(tr).max()
     assert round(pa[0] / p["dt"]) == round(pb[0] / p["dt"]) == round(pc[0] / p["dt"])
     assert abs(pa[0] - pb[0]) < 1e-3 * p["dt"]
