@@ -325,20 +325,33 @@ def _sweep(args):
     torch.cuda.synchronize()
     t_plain = time.perf_counter() - t0
 
-    t0 = time.perf_counter()
-    b = batch.BatchSolver(specs)
+    # warm-up of the batch paths (kernel attributes, graph capture) on two solves
+    wb = batch.BatchSolver(specs[:2])
     try:
-        b.run(0, K)
-        got = b.traces_numpy(K)
+        wb.set_persistent(True)
+        wb.run(0, 4)
+        wb.traces_numpy(4)
     finally:
-        b.close()
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    same = all(np.array_equal(a, g[:K]) for a, g in zip(plain, got))
+        wb.close()
+    t_modes, gots = {}, {}
+    for persistent in (False, True):
+        t0 = time.perf_counter()
+        b = batch.BatchSolver(specs)
+        try:
+            b.set_persistent(persistent)
+            b.run(0, K)
+            gots[persistent] = b.traces_numpy(K)
+        finally:
+            b.close()
+        torch.cuda.synchronize()
+        t_modes[persistent] = time.perf_counter() - t0
+    t_batch, got = min(t_modes.values()), gots[True]
+    same = all(np.array_equal(a, g[:K]) and np.array_equal(g, q) for a, g, q in zip(plain, got, gots[False]))
     return {"metric": "sweep Gcell-updates/s, batched vs plain loop", "unit": "Gcell-updates/s",
             "solves": len(probs), "steps": K, "cells_per_step": cells,
             "plain": cells * K / t_plain / 1e9, "batched": cells * K / t_batch / 1e9,
             "speedup": t_plain / t_batch, "plain_s": t_plain, "batched_s": t_batch,
+            "batched_per_step_s": t_modes[False], "batched_persistent_s": t_modes[True],
             "traces_identical": bool(same),
             "config": {"workload": args.workload, "uneven24": bool(args.uneven),
                        "timing": "wall clock, set-up and trace download included, synchronised"}}
@@ -419,21 +432,28 @@ def _sweep_compact(K, workload="disk_small", n_az=36):
         sv.close()
     torch.cuda.synchronize()
     t_plain = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    b = batch.BatchSolver(_azimuth_specs_device(base, azs))
-    try:
-        b.run(0, K)
-        got = b.traces_numpy(K)
-    finally:
-        b.close()
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    same = all(np.array_equal(a, g[:K]) for a, g in zip(plain, got))
+    def batched(persistent):
+        t0 = time.perf_counter()
+        b = batch.BatchSolver(_azimuth_specs_device(base, azs))
+        try:
+            b.set_persistent(persistent)
+            b.run(0, K)
+            got = b.traces_numpy(K)
+        finally:
+            b.close()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, got
+
+    batched(True)   # warm-up of the batch paths
+    t_step, got_step = batched(False)
+    t_batch, got = batched(True)
+    same = all(np.array_equal(a, g[:K]) and np.array_equal(g, q) for a, g, q in zip(plain, got, got_step))
     out = {"azimuths": n_az, "steps": K, "workload": workload, "cells_per_solve": cells,
            "plain_s": t_plain, "batched_s": t_batch, "speedup": t_plain / t_batch,
-           "traces_identical": bool(same),
+           "batched_per_step_launches_s": t_step, "traces_identical": bool(same),
            "plain": "per azimuth: host rotation of labels and axes, tables, probe, upload, solve, read back",
-           "batched": "labels uploaded once and rotated on the device, one batch of all azimuths"}
+           "batched": "labels uploaded once and rotated on the device, one batch of all azimuths, "
+                      "one persistent launch per graph chunk (per-step launches timed beside it)"}
     # the gradients of the same sweep (misfit against the traces of a
     # perturbed fabric), one at a time and batched
     disk = inversion.Disk(workload, azs, nt=K, dtype="float32", checkpoint_every=200)

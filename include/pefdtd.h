@@ -233,6 +233,16 @@ int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const Pe
 /* Work layout: planes per z-march (0 = 40) and steps per captured graph
  * (0 = keep). Chosen by pefdtd.autotune. */
 int pe_batch_schedule(PeBatch *b, int z_chunk, int chunk_steps);
+/* Persistent batch mode (on = 1): one cooperative launch per graph chunk
+ * advances every batched solve by the chunk's steps, its blocks alternating
+ * a stress and a velocity phase separated by bounded grid-wide barriers
+ * (a timed-out barrier sets PE_ERR_TIMEOUT in pe_batch_status; nothing
+ * hangs). Bit-identical to the per-step launches (on = 0, the default).
+ * FP32 batches of pair-column solves only, else PE_ERR_UNSUPPORTED. The
+ * reference has no counterpart: it runs one solve at a time, one CuPy launch
+ * per kernel and step (sim/pipeline/sweep_runner.py:322-390,
+ * sim/core/fdtd.py:1784-1813). */
+int pe_batch_set_persistent(PeBatch *B, int on);
 int pe_batch_set_wavelet(PeBatch *b, int i, const void *wavelet, int64_t nt);
 /* Advance every solve i over [step_begin, step_end): states[i], traces[i] as
  * in pe_solver_run. Asynchronous on `stream`. */

@@ -2,8 +2,12 @@
 
 Picks, by timing the batch itself on its own device, the planes per z-march
 (the work-item size: shorter marches give more items and better balance
-across the 148 SMs, longer ones spend less on each march's start-up planes)
-and the number of steps per captured CUDA graph. The timed steps advance the
+across the 148 SMs, longer ones spend less on each march's start-up planes),
+the number of steps per captured CUDA graph, and the launch mode: one
+stress and one velocity launch per step, or one persistent launch per graph
+chunk (pefdtd.batch.BatchSolver.set_persistent). The tile shapes are not a
+choice: the pair-column kernels' tiles are fixed by their register and
+shared-memory budget (two 256-thread blocks per SM). The timed steps advance the
 batch's state, which is zeroed afterwards, so tuning leaves a batch exactly
 as it found a fresh one. Results are cached per device and batch signature in
 a JSON file ($PEFDTD_CACHE or ~/.cache/pefdtd/autotune.json).
@@ -66,9 +70,10 @@ def tune_batch(batch, steps=None, use_cache=True):
     """Choose and apply (z_chunk, chunk_steps); returns them with timings."""
     key = batch_key(batch)
     db = _load() if use_cache else {}
-    if use_cache and key in db:
+    if use_cache and key in db and "persistent" in db[key]:
         z, c = db[key]["z_chunk"], db[key]["chunk_steps"]
         batch.schedule(z, c)
+        batch.set_persistent(db[key]["persistent"])
         return db[key]
     maxnt = min(batch.nt)
     nz_max = max(s[0] for s in batch.shapes)
@@ -90,8 +95,17 @@ def tune_batch(batch, steps=None, use_cache=True):
         batch.reset()
     best_c = min(chunk_trials, key=chunk_trials.get) if chunk_trials else 200
     batch.schedule(best_z, best_c)
-    res = dict(z_chunk=best_z, chunk_steps=best_c, ms_per_step_by_z=trials,
-               ms_per_step_by_chunk=chunk_trials)
+    # launch mode at the chosen layout
+    mode_trials = {}
+    if chunk_trials and batch.set_persistent(True):
+        mode_trials["persistent"] = time_steps(batch, best_c)
+        batch.reset()
+        batch.set_persistent(False)
+        mode_trials["per_step"] = chunk_trials[best_c]
+    persistent = bool(mode_trials) and mode_trials["persistent"] < mode_trials["per_step"]
+    batch.set_persistent(persistent)
+    res = dict(z_chunk=best_z, chunk_steps=best_c, persistent=persistent, ms_per_step_by_z=trials,
+               ms_per_step_by_chunk=chunk_trials, ms_per_step_by_mode=mode_trials)
     if use_cache:
         db[key] = res
         _store(db)

@@ -70,6 +70,7 @@ class BatchSolver:
             for c in range(6):
                 self._st[i].s[c] = st[3 + c].data_ptr()
         self.z_chunk, self.chunk_steps = 0, int(chunk_steps)
+        self.persistent = False
         self.nt = [0] * n
         self.traces = [None] * n
         self._tr = (_capi.C.c_void_p * n)()
@@ -91,6 +92,20 @@ class BatchSolver:
     def schedule(self, z_chunk=0, chunk_steps=0):
         _capi.check(self._L.pe_batch_schedule(self._h, int(z_chunk), int(chunk_steps)))
         self.z_chunk, self.chunk_steps = int(z_chunk), int(chunk_steps)
+
+    def set_persistent(self, on=True):
+        """Persistent mode: one cooperative launch per graph chunk advances
+        every batched solve by all the chunk's steps (grid-wide barriers
+        between the stress and velocity phases; bit-identical to the
+        per-step launches). FP32 pair-column batches only: returns whether
+        the mode is on."""
+        rc = self._L.pe_batch_set_persistent(self._h, int(bool(on)))
+        if rc == _capi.PE_ERR_UNSUPPORTED and on:
+            self.persistent = False
+            return False
+        _capi.check(rc)
+        self.persistent = bool(on)
+        return self.persistent
 
     def reset(self):
         for st in self.states:

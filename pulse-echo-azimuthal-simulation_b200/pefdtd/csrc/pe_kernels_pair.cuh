@@ -161,6 +161,21 @@ __device__ __forceinline__ float2 ldg2_stream(const float *p)
     asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "l"(p));
     return v;
 }
+// the same column loads where other blocks of the same launch write the
+// field (the persistent batch kernel): cached in L2 only, the point where
+// the grid barrier makes other blocks' writes visible
+__device__ __forceinline__ float2 ldcg2(const float *p)
+{
+    float2 v;
+    asm volatile("ld.global.cg.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "l"(p) : "memory");
+    return v;
+}
+template <bool COH>
+__device__ __forceinline__ float2 ld2_column(const float *p)
+{
+    if constexpr (COH) return ldcg2(p);
+    else return ldg2_stream(p);
+}
 
 // ======================================================================== stress
 // Tap limits near the grid faces. The reference skips a tap whose reach
@@ -404,7 +419,7 @@ __device__ __forceinline__ bool pair_tile_inside(const StepArgs<float> &A, int b
 // are issued a plane ahead. The caller synchronises the block before a march
 // that follows another. TIN: pair_tile_inside(A, bx, by) holds, and the
 // x / y limits and guards are compile-time constants.
-template <int NC, bool TS, bool TIN>
+template <int NC, bool TS, bool TIN, bool COH = false>
 __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, const StepArgs<float> &A,
                                                   const float *tab, unsigned char *smem, int bx, int by,
                                                   int zb, int ze, PairPhases &ph)
@@ -450,7 +465,7 @@ __device__ __forceinline__ void stress_pair_march(const TmapsPairStress &M, cons
     // z rings (rz[c][k] <-> plane q-4+k, ry/rx[c][k] <-> q-3+k), one plane ahead
     const float *pz = A.v[2] + col, *py = A.v[1] + col, *px = A.v[0] + col;
     auto ld2col = [&](const float *f, int q) -> float2 {
-        return (pair_ok && q >= 0 && q < nz) ? ldg2_stream(f + (long long)q * sz) : make_float2(0.f, 0.f);
+        return (pair_ok && q >= 0 && q < nz) ? ld2_column<COH>(f + (long long)q * sz) : make_float2(0.f, 0.f);
     };
     float2 rz[8], ry[8], rx[8];   // lane pairs (cell 0, cell 1)
 #pragma unroll
@@ -636,6 +651,16 @@ __device__ __forceinline__ void stage_table(float *dst, const float *src, int n_
     const float4 *s4 = reinterpret_cast<const float4 *>(src);
     float4 *d4 = reinterpret_cast<float4 *>(dst);
     for (int i = threadIdx.x; i < n_mat * (TAB36 / 4); i += blockDim.x) d4[i] = __ldg(s4 + i);
+}
+
+// zero the strain planes' pads (read only by cells that are not updated)
+__device__ __forceinline__ void stress_pair_zero_pads(unsigned char *smem)
+{
+    float *gs = reinterpret_cast<float *>(smem + 128) + PS_VSLOT + 2 * PS_SSLOT;
+    for (int i = threadIdx.x; i < PS_RING * 2 * PS_GOFF; i += blockDim.x) {
+        const int p = i / (2 * PS_GOFF), k = i % (2 * PS_GOFF);
+        gs[p * PS_GST + (k < PS_GOFF ? k : PS_GST - 2 * PS_GOFF + k)] = 0.f;
+    }
 }
 
 __device__ __forceinline__ void stress_pair_init(unsigned char *smem)
@@ -831,12 +856,15 @@ __device__ __forceinline__ bool pair_vtile_inside(const StepArgs<float> &A, int 
 // One z-march of a block over cell tile (bx, by), planes [zb, ze); it0 as
 // in stress_pair_march. TIN: pair_vtile_inside(A, bx, by) holds, and the
 // x / y limits and neighbour tests are compile-time constants.
-template <int NC, bool TIN>
+// bars_at: the three mbarriers (default: the first bytes of smem; the
+// persistent batch kernel keeps separate ones for each phase)
+template <int NC, bool TIN, bool COH = false>
 __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, const StepArgs<float> &A,
                                                    const float *rho_tab, unsigned char *smem, int bx,
-                                                   int by, int zb, int ze, int it0)
+                                                   int by, int zb, int ze, int it0,
+                                                   unsigned long long *bars_at = nullptr)
 {
-    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem);
+    unsigned long long *bars = bars_at ? bars_at : reinterpret_cast<unsigned long long *>(smem);
     float *slots = reinterpret_cast<float *>(smem + 128);
     const int tid = threadIdx.x;
     const int l = tid & (PR_LX - 1), r = tid >> 4;
@@ -865,7 +893,7 @@ __device__ __forceinline__ int velocity_pair_march(const TmapsPairVelocity &M, c
     };
     const float *p3 = A.s[2] + col, *p4 = A.s[3] + col, *p5 = A.s[4] + col;
     auto ld2col = [&](const float *f, int z) -> float2 {
-        return (out_ok && z >= 0 && z < nz) ? ldg2_stream(f + (long long)z * sz) : make_float2(0.f, 0.f);
+        return (out_ok && z >= 0 && z < nz) ? ld2_column<COH>(f + (long long)z * sz) : make_float2(0.f, 0.f);
     };
     float2 r3[8], r4[8], r5[8];   // lane pairs: r3[k] <-> z-3+k, r4/r5[k] <-> z-4+k
 #pragma unroll
@@ -1129,6 +1157,127 @@ __global__ void __launch_bounds__(PV_N, 2)
         else
             it0 += velocity_pair_march<NC, false>(maps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, ze, it0);
         cur = w.solve;
+    }
+}
+
+// ---------------------------------------------------------------- persistent batches
+// One launch advances every batched solve by nk steps: the blocks (all
+// resident: a cooperative launch) alternate a stress phase and a velocity
+// phase over the same work items as k_stress_pair_batch /
+// k_velocity_pair_batch, separated by grid-wide barriers. Differences from
+// the per-step launches, each needed because other blocks of the same launch
+// write the fields a block reads:
+//  - the z-ring column loads are L2-coherent (ld.global.cg) instead of the
+//    read-only path;
+//  - after each barrier every thread fences the async proxy, so the TMA
+//    boxes it issues read what the barrier made visible;
+//  - the two phases keep separate mbarriers (stress: bytes 0-23, velocity:
+//    bytes 64-87 of shared memory) and share the data region after them, so
+//    the strain ring's zero pads, the stiffness table and the density table
+//    are restaged at the start of each phase.
+// The arithmetic is the per-step kernels': results are bit-identical.
+constexpr unsigned long long GRID_SPIN_LIMIT = 1ull << 24;   // barrier polls (64 ns sleeps) before giving up
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+
+// Bounded grid-wide barrier: a block's writes, a fence, its arrival; then
+// poll (acquire) until `target` blocks have arrived, at most GRID_SPIN_LIMIT
+// polls, after which it records STATUS_TIMEOUT in the status word and goes
+// on (the results are then invalid; nothing hangs).
+__device__ __forceinline__ void grid_barrier(unsigned *count, unsigned target, int *status)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fence_proxy_async_global();
+        __threadfence();
+        atomicAdd(count, 1u);
+        unsigned long long it = 0;
+        while (ld_acquire_u32(count) < target) {
+            if (++it >= GRID_SPIN_LIMIT) {
+                if (status) atomicExch(status, STATUS_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    fence_proxy_async_global();
+}
+
+__host__ __device__ constexpr size_t persistent_pair_smem(size_t smem_s, size_t smem_v)
+{
+    return smem_s > smem_v ? smem_s : smem_v;
+}
+
+template <int NC, bool TS>
+__global__ void __launch_bounds__(PS_N, 2)
+    k_pair_batch_persistent(const StepArgs<float> *__restrict__ descs, const TmapsPairStress *__restrict__ smaps,
+                            const TmapsPairVelocity *__restrict__ vmaps, const float *const *__restrict__ tabs,
+                            const int *__restrict__ n_mats, const BatchItem *__restrict__ items_s, int n_s,
+                            const BatchItem *__restrict__ items_v, int n_v, int nk, unsigned *bar, int *status)
+{
+    extern __shared__ __align__(128) unsigned char smem_pair[];
+    __shared__ __align__(16) StepArgs<float> As;
+    unsigned long long *vbars = reinterpret_cast<unsigned long long *>(smem_pair) + 8;
+    float *tsm = reinterpret_cast<float *>(smem_pair + PS_SMEM_FIXED);
+    float *rsm = reinterpret_cast<float *>(smem_pair + 128) + 3 * PV_SLOT;
+    stress_pair_init(smem_pair);
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 3; ++b) mbar_init(vbars + b, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const int per_s = (n_s + gridDim.x - 1) / gridDim.x, i0s = blockIdx.x * per_s, i1s = min(n_s, i0s + per_s);
+    const int per_v = (n_v + gridDim.x - 1) / gridDim.x, i0v = blockIdx.x * per_v, i1v = min(n_v, i0v + per_v);
+    PairPhases ph{0, 0};
+    int it0 = 0;
+    unsigned nbar = 0;
+    for (int k = 0; k < nk; ++k) {
+        int cur = -1;
+        for (int it = i0s; it < i1s; ++it) {
+            const BatchItem w = items_s[it];
+            __syncthreads();   // the previous march is finished by every thread
+            if (w.solve != cur) {
+                copy_args(&As, descs + w.solve, k);
+                if (TS) stage_table(tsm, tabs[w.solve], n_mats[w.solve]);
+            }
+            __syncthreads();
+            const int zb = w.bz * As.zc, ze = min(zb + As.zc, As.nz);
+            const float *tab = TS ? tsm : tabs[w.solve];
+            if (pair_tile_inside(As, w.bx, w.by))
+                stress_pair_march<NC, TS, true, true>(smaps[w.solve], As, tab, smem_pair, w.bx, w.by, zb, ze, ph);
+            else
+                stress_pair_march<NC, TS, false, true>(smaps[w.solve], As, tab, smem_pair, w.bx, w.by, zb, ze, ph);
+            cur = w.solve;
+        }
+        grid_barrier(bar, ++nbar * gridDim.x, status);
+        cur = -1;
+        for (int it = i0v; it < i1v; ++it) {
+            const BatchItem w = items_v[it];
+            __syncthreads();
+            if (w.solve != cur) {
+                copy_args(&As, descs + w.solve, k);
+                for (int i = threadIdx.x; i < n_mats[w.solve]; i += PV_N) rsm[i] = As.rho[i];
+            }
+            __syncthreads();
+            const int zb = w.bz * As.zc, ze = min(zb + As.zc, As.nz);
+            if (pair_vtile_inside(As, w.bx, w.by))
+                it0 += velocity_pair_march<NC, true, true>(vmaps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, ze,
+                                                           it0, vbars);
+            else
+                it0 += velocity_pair_march<NC, false, true>(vmaps[w.solve], As, rsm, smem_pair, w.bx, w.by, zb, ze,
+                                                            it0, vbars);
+            cur = w.solve;
+        }
+        grid_barrier(bar, ++nbar * gridDim.x, status);
+        stress_pair_zero_pads(smem_pair);   // the velocity slots overwrote them
     }
 }
 

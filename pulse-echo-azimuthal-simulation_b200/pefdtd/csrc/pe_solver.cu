@@ -1086,13 +1086,19 @@ struct PeBatch {
     pe::TmapsPairStress *pmaps_s = nullptr;
     pe::TmapsPairVelocity *pmaps_v = nullptr;
     const float **tabs = nullptr;
+    // persistent mode: one cooperative launch per graph chunk runs every step
+    // of the batched pair solves (k_pair_batch_persistent)
+    bool persistent = false;
+    unsigned *bar = nullptr;        // grid barrier counter, zeroed before each launch
+    int grid_p = 1;
+    size_t smem_p = 0;
 
     ~PeBatch()
     {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (stream) cudaStreamSynchronize(stream);
         for (PeSolver *s : solves) pe_solver_destroy(s);
-        void *bufs[] = {step, status, descs, maps_s, maps_v, nmats, items_s, items_v, pmaps_s, pmaps_v, tabs};
+        void *bufs[] = {step, status, descs, maps_s, maps_v, nmats, items_s, items_v, pmaps_s, pmaps_v, tabs, bar};
         for (void *b : bufs)
             if (b) cudaFree(b);
         if (ev_in) cudaEventDestroy(ev_in);
@@ -1150,6 +1156,11 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
     PE_CUDA(setattr((const void *)pe::k_stress_pair_batch<0, false>));
     PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<4>));
     PE_CUDA(setattr((const void *)pe::k_velocity_pair_batch<0>));
+    PE_CUDA(setattr((const void *)pe::k_pair_batch_persistent<4, true>));
+    PE_CUDA(setattr((const void *)pe::k_pair_batch_persistent<4, false>));
+    PE_CUDA(setattr((const void *)pe::k_pair_batch_persistent<0, true>));
+    PE_CUDA(setattr((const void *)pe::k_pair_batch_persistent<0, false>));
+    B->smem_p = pe::persistent_pair_smem(B->smem_s, B->smem_v);
     for (int s = 0; s < (int)B->solves.size(); ++s) {
         PeSolver *S = B->solves[s];
         if (!batched(B, S)) continue;
@@ -1163,11 +1174,16 @@ int batch_layout_pair(PeBatch *B, int nsm, int optin, std::vector<pe::BatchItem>
                 for (int bx = 0; bx < (c.nx + pe::PV_OX - 1) / pe::PV_OX; ++bx) iv.push_back({s, bx, by, bz});
         }
     }
-    int per_v = 1, per_s = 1;
+    int per_v = 1, per_s = 1, per_p = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_v, pe::k_velocity_pair_batch<4>, pe::PV_N, B->smem_v);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_s, pe::k_stress_pair_batch<4, true>, pe::PS_N, B->smem_s);
     B->grid_s = std::max(1, std::min((int)is.size(), nsm * std::max(1, per_s)));
     B->grid_v = std::max(1, std::min((int)iv.size(), nsm * std::max(1, per_v)));
+    // the persistent kernel's blocks must all be resident at once (its grid
+    // barriers wait for every block): at most the occupancy times the SMs
+    PE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_p, pe::k_pair_batch_persistent<4, true>, pe::PS_N,
+                                                          B->smem_p));
+    B->grid_p = std::max(1, std::min((int)std::max(is.size(), iv.size()), nsm * std::max(1, per_p)));
     return PE_OK;
 }
 
@@ -1299,13 +1315,55 @@ int batch_upload(PeBatch *B, const PeState *states, void *const *traces)
     return PE_OK;
 }
 
+// the persistent batch kernel over `len` steps (a cooperative launch: the
+// runtime refuses it rather than leave any block unresident)
+int launch_pair_persistent(PeBatch *B, int len)
+{
+    PE_CUDA(cudaMemsetAsync(B->bar, 0, sizeof(unsigned), B->stream));
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)B->grid_p, 1, 1);
+    lc.blockDim = dim3(pe::PS_N, 1, 1);
+    lc.dynamicSmemBytes = B->smem_p;
+    lc.stream = B->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    const pe::StepArgs<float> *d = (const pe::StepArgs<float> *)B->descs;
+    const float *const *tabs = B->tabs;
+    const pe::TmapsPairStress *ms = B->pmaps_s;
+    const pe::TmapsPairVelocity *mv = B->pmaps_v;
+    const int *nm = B->nmats;
+    const pe::BatchItem *is = B->items_s, *iv = B->items_v;
+    const int ns = B->n_items_s, nv = B->n_items_v;
+    cudaError_t e;
+    if (B->pair_nc4 && B->pair_ts)
+        e = cudaLaunchKernelEx(&lc, pe::k_pair_batch_persistent<4, true>, d, ms, mv, tabs, nm, is, ns, iv, nv, len, B->bar, B->status);
+    else if (B->pair_nc4)
+        e = cudaLaunchKernelEx(&lc, pe::k_pair_batch_persistent<4, false>, d, ms, mv, tabs, nm, is, ns, iv, nv, len, B->bar, B->status);
+    else if (B->pair_ts)
+        e = cudaLaunchKernelEx(&lc, pe::k_pair_batch_persistent<0, true>, d, ms, mv, tabs, nm, is, ns, iv, nv, len, B->bar, B->status);
+    else
+        e = cudaLaunchKernelEx(&lc, pe::k_pair_batch_persistent<0, false>, d, ms, mv, tabs, nm, is, ns, iv, nv, len, B->bar, B->status);
+    if (e != cudaSuccess) return fail(PE_ERR_CUDA, std::string("persistent batch launch: ") + cudaGetErrorString(e));
+    B->launches += 1;
+    return PE_OK;
+}
+
 template <typename T>
 int batch_chunk(PeBatch *B, int len)
 {
     const dim3 block(pe::TB_X, pe::TB_Y, 1);
+    if constexpr (std::is_same<T, float>::value) {
+        if (B->pair_batch && B->persistent && B->n_items_s > 0) {
+            const int rc = launch_pair_persistent(B, len);
+            if (rc) return rc;
+        }
+    }
     for (int k = 0; k < len; ++k) {
         if constexpr (std::is_same<T, float>::value) {
-            if (B->pair_batch && B->n_items_s > 0) {
+            if (B->pair_batch && !B->persistent && B->n_items_s > 0) {
                 const pe::StepArgs<float> *d = (const pe::StepArgs<float> *)B->descs;
                 const int ns = B->n_items_s, nv = B->n_items_v;
                 if (B->pair_nc4 && B->pair_ts)
@@ -1423,6 +1481,7 @@ int pe_batch_create(int n, const PeConfig *cfgs, const PeMedium *media, const Pe
     if ((rc = dev_alloc(&B->step, sizeof(long long)))) return rc;
     if ((rc = dev_alloc(&B->status, sizeof(int)))) return rc;
     PE_CUDA(cudaMemset(B->status, 0, sizeof(int)));
+    if ((rc = dev_alloc(&B->bar, sizeof(unsigned)))) return rc;
     const size_t ds = B->dtype == PE_F64 ? sizeof(pe::StepArgs<double>) : sizeof(pe::StepArgs<float>);
     if ((rc = dev_alloc(&B->descs, ds * n))) return rc;
     if ((rc = dev_alloc(&B->maps_s, sizeof(pe::TmapsStress) * n))) return rc;
@@ -1451,6 +1510,21 @@ int pe_batch_schedule(PeBatch *B, int z_chunk, int chunk_steps)
     for (PeSolver *S : B->solves) S->cfg.z_chunk = 0;
     B->uploaded = false;
     return B->dtype == PE_F64 ? batch_layout<double>(B) : batch_layout<float>(B);
+}
+
+int pe_batch_set_persistent(PeBatch *B, int on)
+{
+    if (!B) return fail(PE_ERR_INVALID, "null batch");
+    if (on && !B->pair_batch)
+        return fail(PE_ERR_UNSUPPORTED, "the persistent kernel runs FP32 batches of pair-column solves");
+    if (B->persistent != (on != 0)) {
+        B->persistent = on != 0;
+        if (B->gexec) {
+            cudaGraphExecDestroy(B->gexec);
+            B->gexec = nullptr;
+        }
+    }
+    return PE_OK;
 }
 
 int pe_batch_set_wavelet(PeBatch *B, int i, const void *wavelet, int64_t nt)

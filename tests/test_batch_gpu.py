@@ -152,3 +152,41 @@ def test_batch_mixing_solo_and_shared_solves():
         ref = O.run_oracle(oracle_prob(p, record=p["record"], damped_record=True), fma_mode=1)
         assert np.abs(ref).max() > 0
         assert np.array_equal(tr, ref)
+
+
+@pytest.mark.parametrize("case", ["mixed", "large_table_orders", "with_solo"])
+def test_persistent_batch_equals_per_step_launches(case):
+    """One cooperative launch per graph chunk (every step of the batched
+    solves, grid barriers between the phases) gives the per-step launches'
+    traces and final states bit for bit, on fewer launches; a partial chunk
+    (not captured) too."""
+    from pefdtd import batch
+    from pefdtd.coeffs import optimised_coeffs
+    if case == "mixed":
+        probs, nt, kw = _problems(), 90, dict(z_chunk=7, chunk_steps=40)
+    elif case == "large_table_orders":
+        a = dict(make_small(nt=60, shape=(14, 40, 40), n_grains=600, sponge=2, seed=21))
+        b6 = dict(make_small(nt=60, shape=(16, 36, 44), n_grains=7, sponge=2, seed=22))
+        b6["coeffs"] = optimised_coeffs(6)
+        probs, nt, kw = [a, b6], 60, dict(z_chunk=5, chunk_steps=25)
+    else:
+        probs = [make_small(nt=40, shape=(40, 256, 256), n_grains=300, sponge=4, seed=31),
+                 make_small(nt=40, shape=(20, 28, 32), n_grains=5, sponge=3, seed=32)]
+        nt, kw = 40, dict(chunk_steps=20)
+    out = {}
+    for persistent in (False, True):
+        b = batch.BatchSolver([batch.spec_from_problem(p) for p in probs], **kw)
+        try:
+            assert b.set_persistent(persistent) == persistent
+            b.run(0, nt - 7)
+            b.run(nt - 7, nt)
+            out[persistent] = (b.traces_numpy(nt), [s.cpu().numpy() for s in b.states], b.launch_count())
+        finally:
+            b.close()
+    (t0, s0, l0), (t1, s1, l1) = out[False], out[True]
+    for a, c in zip(t0, t1):
+        assert np.abs(a).max() > 0
+        assert np.array_equal(a, c)
+    for a, c in zip(s0, s1):
+        assert np.array_equal(a.view(np.uint32), c.view(np.uint32))
+    assert l1 < l0
