@@ -168,15 +168,21 @@ int pe_solver_profile(PeSolver *s, const PeState *state, int n_steps, float *ms_
 int pe_solver_destroy(PeSolver *s);
 
 /* One call, host buffers in and out: the reference's forward_fused_labels
- * contract for callers without device memory management. Allocates the
- * state on the device, zeroes it, runs nt steps and copies the (nt, n_groups)
- * traces (dtype) back into traces_host. labels_host is (nz, ny, nx) uint16,
- * damp_volume_host f32 or NULL; medium->labels_dev/damp_volume_dev are
- * ignored. */
+ * contract (sim/core/fdtd.py:1618-1816) for callers without device memory
+ * management. Uploads the labels, zeroes the state on the device, runs nt
+ * steps and copies the (nt, n_groups) traces (dtype) back into traces_host.
+ * labels_host is (nz, ny, nx) uint16, damp_volume_host f32 or NULL;
+ * medium->labels_dev/damp_volume_dev are ignored. The device buffers (state,
+ * labels, damping, traces) are kept per device between calls, grown when a
+ * call needs more, so that repeated calls allocate nothing; calls on one
+ * device run one at a time. */
 int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host,
                     const float *damp_volume_host, const PeMedium *medium,
                     const PeProbe *probe, const void *wavelet_host, int64_t nt,
                     void *traces_host);
+/* Free the device buffers pe_forward_host keeps (every device). No
+ * reference counterpart. */
+void pe_forward_host_release(void);
 
 /* ---- Adjoint ---------------------------------------------------------------
  * One reverse step of the exact discrete adjoint of pe_solver_run's step n

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <type_traits>
@@ -988,6 +989,39 @@ int pe_solver_destroy(PeSolver *S)
     return PE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Device buffers of pe_forward_host kept between calls, per device
+// (grow-only): a call of the same or a smaller size allocates and frees
+// nothing, and so does not pay cudaMalloc / cudaFree (whose synchronisation
+// and mapping of a 377 MB state dominate a short call). Released by
+// pe_forward_host_release.
+struct HostEntryBufs {
+    std::mutex mu;
+    void *lab = nullptr, *dvol = nullptr, *fields = nullptr, *traces = nullptr;
+    size_t c_lab = 0, c_dvol = 0, c_fields = 0, c_traces = 0;
+    cudaStream_t st = nullptr;
+};
+constexpr int HOST_ENTRY_DEVICES = 64;
+HostEntryBufs g_host_bufs[HOST_ENTRY_DEVICES];
+
+int grow(void **p, size_t *cap, size_t need)
+{
+    if (need <= *cap) return PE_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    const int rc = dev_alloc(p, need);
+    if (rc == PE_OK) *cap = need;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
 int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host, const float *damp_host,
                     const PeMedium *medium, const PeProbe *probe, const void *wavelet_host,
                     int64_t nt, void *traces_host)
@@ -997,39 +1031,42 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host, const floa
     const long long ncell = (long long)cfg->nz * cfg->ny * cfg->nx;
     if (ncell <= 0) return fail(PE_ERR_INVALID, "grid dimensions must be positive");
     const int es = dtype_size(cfg->dtype);
-    uint16_t *lab = nullptr;
-    float *dvol = nullptr;
-    void *fields = nullptr, *traces = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= HOST_ENTRY_DEVICES)
+        return fail(PE_ERR_CUDA, "no usable current device");
+    HostEntryBufs &H = g_host_bufs[dev];
+    std::lock_guard<std::mutex> guard(H.mu);   // calls on one device share the buffers: one at a time
     PeSolver *S = nullptr;
     int rc = PE_OK;
-    cudaStream_t st = nullptr;
     PeMedium md = *medium;
     PeState state{};
     const size_t tr_bytes = (size_t)es * (size_t)std::max<int64_t>(1, nt) * std::max(1, probe->n_groups);
     do {
-        if ((rc = dev_alloc(&lab, sizeof(uint16_t) * ncell))) break;
-        if (damp_host && (rc = dev_alloc(&dvol, sizeof(float) * ncell))) break;
-        if ((rc = dev_alloc(&fields, (size_t)es * 9 * ncell))) break;
-        if ((rc = dev_alloc(&traces, tr_bytes))) break;
-        cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(lab, labels_host, sizeof(uint16_t) * ncell, cudaMemcpyHostToDevice, st);
-        if (ce == cudaSuccess && dvol)
-            ce = cudaMemcpyAsync(dvol, damp_host, sizeof(float) * ncell, cudaMemcpyHostToDevice, st);
-        if (ce == cudaSuccess) ce = cudaMemsetAsync(fields, 0, (size_t)es * 9 * ncell, st);
+        if ((rc = grow(&H.lab, &H.c_lab, sizeof(uint16_t) * ncell))) break;
+        if (damp_host && (rc = grow(&H.dvol, &H.c_dvol, sizeof(float) * ncell))) break;
+        if ((rc = grow(&H.fields, &H.c_fields, (size_t)es * 9 * ncell))) break;
+        if ((rc = grow(&H.traces, &H.c_traces, tr_bytes))) break;
+        cudaError_t ce = cudaSuccess;
+        if (!H.st) ce = cudaStreamCreateWithFlags(&H.st, cudaStreamNonBlocking);
+        cudaStream_t st = H.st;
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(H.lab, labels_host, sizeof(uint16_t) * ncell, cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess && damp_host)
+            ce = cudaMemcpyAsync(H.dvol, damp_host, sizeof(float) * ncell, cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(H.fields, 0, (size_t)es * 9 * ncell, st);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) {
             rc = fail(PE_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce));
             break;
         }
-        md.labels_dev = lab;
-        md.damp_volume_dev = dvol;
+        md.labels_dev = (const uint16_t *)H.lab;
+        md.damp_volume_dev = damp_host ? (const float *)H.dvol : nullptr;
         if ((rc = pe_solver_create(cfg, &md, probe, &S))) break;
         if ((rc = pe_solver_set_wavelet(S, wavelet_host, nt))) break;
-        for (int i = 0; i < 3; ++i) state.v[i] = (char *)fields + (size_t)es * i * ncell;
-        for (int i = 0; i < 6; ++i) state.s[i] = (char *)fields + (size_t)es * (3 + i) * ncell;
-        if ((rc = pe_solver_run(S, &state, traces, 0, nt, st))) break;
+        for (int i = 0; i < 3; ++i) state.v[i] = (char *)H.fields + (size_t)es * i * ncell;
+        for (int i = 0; i < 6; ++i) state.s[i] = (char *)H.fields + (size_t)es * (3 + i) * ncell;
+        if ((rc = pe_solver_run(S, &state, H.traces, 0, nt, st))) break;
         if (probe->n_groups > 0 && nt > 0) {
-            ce = cudaMemcpyAsync(traces_host, traces, (size_t)es * nt * probe->n_groups, cudaMemcpyDeviceToHost, st);
+            ce = cudaMemcpyAsync(traces_host, H.traces, (size_t)es * nt * probe->n_groups, cudaMemcpyDeviceToHost, st);
             if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
             if (ce != cudaSuccess) {
                 rc = fail(PE_ERR_CUDA, std::string("download: ") + cudaGetErrorString(ce));
@@ -1037,13 +1074,24 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host, const floa
             }
         }
     } while (0);
+    if (H.st) cudaStreamSynchronize(H.st);
     if (S) pe_solver_destroy(S);
-    if (st) cudaStreamSynchronize(st), cudaStreamDestroy(st);
-    if (lab) cudaFree(lab);
-    if (dvol) cudaFree(dvol);
-    if (fields) cudaFree(fields);
-    if (traces) cudaFree(traces);
     return rc;
+}
+
+void pe_forward_host_release(void)
+{
+    for (HostEntryBufs &H : g_host_bufs) {
+        std::lock_guard<std::mutex> guard(H.mu);
+        if (H.st) cudaStreamSynchronize(H.st);
+        void *bufs[] = {H.lab, H.dvol, H.fields, H.traces};
+        for (void *b : bufs)
+            if (b) cudaFree(b);
+        H.lab = H.dvol = H.fields = H.traces = nullptr;
+        H.c_lab = H.c_dvol = H.c_fields = H.c_traces = 0;
+        if (H.st) cudaStreamDestroy(H.st);
+        H.st = nullptr;
+    }
 }
 
 }  // extern "C"
