@@ -157,6 +157,47 @@ def test_matches_reference_ringfwi_gradient():
     assert np.linalg.norm(ours - ref) <= 1e-8 * np.linalg.norm(ref)
 
 
+def test_matches_reference_ringfwi_gradient_on_disk_small_copy():
+    """The same comparison on the 96 x 96 x 64 copy of the gradient
+    configuration: the disk_small specimen (50 grains, the workload's labels),
+    300 steps, misfit against the c-axes re-drawn with the next seed
+    (tests/golden/make_adjoint_disk_small.py); gradients with respect to all
+    100 per-grain angles. Checkpoints every 64 steps with two-level
+    recomputation, as a large solve would run."""
+    import torch
+    from golden.make_adjoint_disk_small import label_digest
+    from pefdtd import workloads
+    from pefdtd.adjoint import Problem, angles_from_axes, ice_table21
+    path = os.path.join(GOLD, "adjoint_disk_small.npz")
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    g = np.load(path)
+    nt = int(g["nt"])
+    p = workloads.make_problem("disk_small", nt=nt)
+    assert label_digest(p["lab"]) == str(g["digest"])
+    th0, ph0 = angles_from_axes(p["axes"])
+    assert np.array_equal(th0, g["theta"]) and np.array_equal(ph0, g["phi"])
+    lab = p["lab"]
+    n_mat = int(lab.max()) + 2
+    pts = [tuple(q) for q in g["pts"]]
+    w = 1.0 / len(pts)
+    prob = Problem((lab + 1).astype(np.uint16), np.full(n_mat, 917.0), float(g["h"]), float(g["dt"]),
+                   [1.0], [(q, w) for q in pts], [(pts, [w] * len(pts))], g["wavelet"],
+                   record="pressure", sponge_width=0, damped_record=False, dtype="float64",
+                   checkpoint_every=64, inner_every=9)
+    th = torch.tensor(g["theta"], requires_grad=True)
+    ph = torch.tensor(g["phi"], requires_grad=True)
+    tr = prob.traces(ice_table21(th, ph, c_couplant=1500.0, rho_couplant=917.0))
+    J = 0.5 * ((tr - torch.tensor(g["dobs"])) ** 2).sum()
+    J.backward()
+    assert float(g["J"]) > 0
+    assert abs(float(J.detach()) - float(g["J"])) <= 1e-9 * float(g["J"])
+    ours = np.concatenate([th.grad.numpy(), ph.grad.numpy()])
+    ref = np.concatenate([g["g_theta"], g["g_phi"]])
+    assert np.count_nonzero(ref) > 0.5 * len(ref)
+    assert np.linalg.norm(ours - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
 def test_misfit_gradients_batched_equal_one_at_a_time(dtype):
     """Several solves of different grids, their segments interleaved on one
