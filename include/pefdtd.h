@@ -180,9 +180,13 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host,
                     const float *damp_volume_host, const PeMedium *medium,
                     const PeProbe *probe, const void *wavelet_host, int64_t nt,
                     void *traces_host);
-/* Free the device buffers pe_forward_host keeps (every device). No
+/* Give back to the driver the device memory the library keeps for reuse:
+ * pe_forward_host's buffers and the cache of freed solver and batch buffers
+ * (a destroyed solve's buffers are kept, up to 8 GiB per device, and reused
+ * by a later solve of the same sizes, so that repeated solves allocate and
+ * free nothing). Call with no solve, batch or host-entry call in flight. No
  * reference counterpart. */
-void pe_forward_host_release(void);
+void pe_release_cached_memory(void);
 
 /* ---- Adjoint ---------------------------------------------------------------
  * One reverse step of the exact discrete adjoint of pe_solver_run's step n

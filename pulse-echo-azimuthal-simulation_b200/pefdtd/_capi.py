@@ -135,7 +135,7 @@ def exported_symbols():
     return ["pe_abi_version", "pe_last_error", "pe_solver_create", "pe_solver_set_wavelet",
             "pe_solver_run", "pe_solver_launch_count", "pe_solver_profile", "pe_solver_status",
             "pe_solver_destroy",
-            "pe_forward_host", "pe_forward_host_release", "pe_label_cylinder", "pe_rotated_grid", "pe_batch_create", "pe_batch_schedule", "pe_batch_set_persistent",
+            "pe_forward_host", "pe_release_cached_memory", "pe_label_cylinder", "pe_rotated_grid", "pe_batch_create", "pe_batch_schedule", "pe_batch_set_persistent",
             "pe_batch_set_wavelet", "pe_batch_run", "pe_batch_status", "pe_batch_launch_count",
             "pe_batch_destroy", "pe_trace_envelope", "pe_trace_detrend", "pe_trace_pick",
             "pe_trace_analyse"]

@@ -16,6 +16,7 @@
 #include <memory>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "pe_kernels.cuh"
@@ -43,16 +44,96 @@ int fail(int code, const std::string &msg)
                         std::string(#expr) + ": " + cudaGetErrorString(e_));               \
     } while (0)
 
+// Device buffers of solvers, batches and the host entry come from a
+// per-device cache: a freed buffer is kept and handed out again for a request
+// of the same size (rounded to 256 bytes), so that creating and destroying
+// solves of the same shapes allocates and frees nothing after the first
+// time. cudaMalloc and cudaFree synchronise the device, and cudaFree of a
+// large buffer can stall for much longer. At most POOL_KEEP bytes are kept
+// per device (beyond that a freed buffer goes back to the driver);
+// pe_release_cached_memory empties the cache. Buffers are returned only
+// after the work using them has finished (their owners synchronise first).
+constexpr int POOL_DEVICES = 64;
+constexpr size_t POOL_KEEP = (size_t)8 << 30;
+struct DevPool {
+    std::mutex mu;
+    std::unordered_map<void *, size_t> live;   // handed out: size
+    std::multimap<size_t, void *> idle;        // kept for reuse
+    size_t idle_bytes = 0;
+};
+DevPool g_pool[POOL_DEVICES];
+
+DevPool *pool_of_current()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= POOL_DEVICES) return nullptr;
+    return &g_pool[dev];
+}
+
 template <typename P>
 int dev_alloc(P **p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    DevPool *pool = pool_of_current();
+    if (pool) {
+        std::lock_guard<std::mutex> g(pool->mu);
+        auto it = pool->idle.find(bytes);
+        if (it != pool->idle.end()) {
+            *p = (P *)it->second;
+            pool->idle_bytes -= bytes;
+            pool->idle.erase(it);
+            pool->live[(void *)*p] = bytes;
+            return PE_OK;
+        }
+    }
     cudaError_t e = cudaMalloc((void **)p, bytes);
-    if (e != cudaSuccess)
+    if (e != cudaSuccess) {
+        *p = nullptr;
         return fail(PE_ERR_NOMEM, std::string("cudaMalloc(") + std::to_string(bytes) +
                                       "): " + cudaGetErrorString(e));
+    }
+    if (pool) {
+        std::lock_guard<std::mutex> g(pool->mu);
+        pool->live[(void *)*p] = bytes;
+    }
     return PE_OK;
+}
+
+// return a dev_alloc buffer to the cache of the device it came from (the
+// current device's cache is searched first, then the others)
+void dev_free(void *p)
+{
+    if (!p) return;
+    DevPool *cur = pool_of_current();
+    for (int d = -1; d < POOL_DEVICES; ++d) {
+        DevPool *pool = d < 0 ? cur : &g_pool[d];
+        if (!pool || (d >= 0 && pool == cur)) continue;
+        std::lock_guard<std::mutex> g(pool->mu);
+        auto it = pool->live.find(p);
+        if (it == pool->live.end()) continue;
+        const size_t bytes = it->second;
+        pool->live.erase(it);
+        if (pool->idle_bytes + bytes <= POOL_KEEP) {
+            pool->idle.emplace(bytes, p);
+            pool->idle_bytes += bytes;
+        } else {
+            cudaFree(p);
+        }
+        return;
+    }
+    cudaFree(p);
+}
+
+void pool_release_all()
+{
+    for (DevPool &pool : g_pool) {
+        std::lock_guard<std::mutex> g(pool.mu);
+        for (auto &kv : pool.idle) cudaFree(kv.second);
+        pool.idle.clear();
+        pool.idle_bytes = 0;
+    }
 }
 
 int dtype_size(int dtype) { return dtype == PE_F64 ? 8 : 4; }
@@ -123,7 +204,7 @@ struct PeSolver {
         void *bufs[] = {lab, c21, rho, dz, dy, dx, dvol, src_idx, src_w, rec_cell,
                         rec_pos, rec_w, grp_off, rec_val, wavelet, step, status, ent_group, tab36, rinv, grad_rep};
         for (void *b : bufs)
-            if (b) cudaFree(b);
+            if (b) dev_free(b);
     }
 };
 
@@ -620,7 +701,7 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
     unsigned long long bad = 0;
     PE_CUDA(cudaMemcpyAsync(&bad, nbad, sizeof(bad), cudaMemcpyDeviceToHost, st));
     PE_CUDA(cudaStreamSynchronize(st));
-    cudaFree(nbad);
+    dev_free(nbad);
     if (bad)
         return fail(PE_ERR_INVALID, std::to_string(bad) + " cells carry a material index >= n_mat (" +
                                         std::to_string(c.n_mat) + "): label has no table row");
@@ -642,7 +723,7 @@ int pe_solver_create(const PeConfig *cfg, const PeMedium *md, const PeProbe *pr,
             pe::k_rho_inv<<<(c.n_mat + 127) / 128, 128, 0, st>>>((const float *)S->rho, S->rinv, c.n_mat);
         }
         PE_CUDA(cudaStreamSynchronize(st));
-        cudaFree(c36);
+        dev_free(c36);
     }
     if (all_sp) {
         if ((rc = dev_alloc(&S->dz, sizeof(float) * c.nz))) return rc;
@@ -697,7 +778,7 @@ int pe_solver_set_wavelet(PeSolver *S, const void *wavelet, int64_t nt)
 {
     if (!S || (nt > 0 && !wavelet) || nt < 0) return fail(PE_ERR_INVALID, "bad wavelet");
     if (S->wavelet) {
-        cudaFree(S->wavelet);
+        dev_free(S->wavelet);
         S->wavelet = nullptr;
     }
     int rc = dev_alloc(&S->wavelet, (size_t)S->esize * std::max<int64_t>(1, nt));
@@ -983,7 +1064,10 @@ int pe_solver_profile(PeSolver *S, const PeState *state, int n_steps, float *ms_
 int pe_solver_destroy(PeSolver *S)
 {
     if (S) {
-        cudaStreamSynchronize(S->stream);
+        // the solve's buffers go back to the cache for reuse: every stream's
+        // work on them (runs, adjoint segments on the caller's stream) must
+        // be finished first, as cudaFree's implicit synchronisation ensured
+        cudaDeviceSynchronize();
         delete S;
     }
     return PE_OK;
@@ -997,7 +1081,7 @@ namespace {
 // (grow-only): a call of the same or a smaller size allocates and frees
 // nothing, and so does not pay cudaMalloc / cudaFree (whose synchronisation
 // and mapping of a 377 MB state dominate a short call). Released by
-// pe_forward_host_release.
+// pe_release_cached_memory.
 struct HostEntryBufs {
     std::mutex mu;
     void *lab = nullptr, *dvol = nullptr, *fields = nullptr, *traces = nullptr;
@@ -1010,7 +1094,7 @@ HostEntryBufs g_host_bufs[HOST_ENTRY_DEVICES];
 int grow(void **p, size_t *cap, size_t need)
 {
     if (need <= *cap) return PE_OK;
-    if (*p) cudaFree(*p);
+    if (*p) dev_free(*p);
     *p = nullptr;
     *cap = 0;
     const int rc = dev_alloc(p, need);
@@ -1079,19 +1163,20 @@ int pe_forward_host(const PeConfig *cfg, const uint16_t *labels_host, const floa
     return rc;
 }
 
-void pe_forward_host_release(void)
+void pe_release_cached_memory(void)
 {
     for (HostEntryBufs &H : g_host_bufs) {
         std::lock_guard<std::mutex> guard(H.mu);
         if (H.st) cudaStreamSynchronize(H.st);
         void *bufs[] = {H.lab, H.dvol, H.fields, H.traces};
         for (void *b : bufs)
-            if (b) cudaFree(b);
+            if (b) dev_free(b);
         H.lab = H.dvol = H.fields = H.traces = nullptr;
         H.c_lab = H.c_dvol = H.c_fields = H.c_traces = 0;
         if (H.st) cudaStreamDestroy(H.st);
         H.st = nullptr;
     }
+    pool_release_all();
 }
 
 }  // extern "C"
@@ -1148,7 +1233,7 @@ struct PeBatch {
         for (PeSolver *s : solves) pe_solver_destroy(s);
         void *bufs[] = {step, status, descs, maps_s, maps_v, nmats, items_s, items_v, pmaps_s, pmaps_v, tabs, bar};
         for (void *b : bufs)
-            if (b) cudaFree(b);
+            if (b) dev_free(b);
         if (ev_in) cudaEventDestroy(ev_in);
         if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
@@ -1303,8 +1388,8 @@ int batch_layout(PeBatch *B)
     }
     B->n_items_s = (int)is.size();
     B->n_items_v = (int)iv.size();
-    if (B->items_s) cudaFree(B->items_s);
-    if (B->items_v) cudaFree(B->items_v);
+    if (B->items_s) dev_free(B->items_s);
+    if (B->items_v) dev_free(B->items_v);
     B->items_s = B->items_v = nullptr;
     int rc;
     if ((rc = dev_alloc(&B->items_s, sizeof(pe::BatchItem) * is.size()))) return rc;
