@@ -80,9 +80,10 @@ def top_probe(lab, h, aperture):
     iz = int(ice_z[0])
     r = aperture / 2
     yc, xc = (ny - 1) / 2, (nx - 1) / 2
-    pts = [(iz, iy, ix) for iy in range(ny) for ix in range(nx)
-           if ((iy - yc) * h) ** 2 + ((ix - xc) * h) ** 2 <= r * r and lab[iz, iy, ix] >= 0]
-    return pts
+    Y, X = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    inside = (((Y - yc) * h) ** 2 + ((X - xc) * h) ** 2 <= r * r) & (lab[iz] >= 0)
+    iy, ix = np.nonzero(inside)            # row-major: the order of the (iy, ix) loop
+    return [(iz, int(a), int(b)) for a, b in zip(iy, ix)]
 
 
 def make_problem(name_or_spec, nt=None, use_gpu=None, kh_max=2.0):
