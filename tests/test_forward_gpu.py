@@ -143,7 +143,8 @@ def test_many_materials_vs_reference_dense():
 def test_disk_small_workload_parity_and_picks():
     """The benchmark's small configuration (64 x 96 x 96, 50 grains), 600
     steps: bit-exact vs the oracle, within 1e-5 of the reference kernels,
-    same echo pick."""
+    same pick of the transmitted burst (the full-length runs and the
+    bottom-echo picks are in test_echo_parity_gpu.py)."""
     from pefdtd import workloads, wavelets
     p = workloads.make_problem("disk_small", nt=600)
     tr = _fwd(p, record="vz", damped_record=True)
@@ -220,13 +221,12 @@ def test_progress_callback_cadence_and_abort():
         _fwd(p, progress=stop)
 
 
-def test_host_entry_matches_device_path():
-    """pe_forward_host (host buffers in and out) == DeviceSolve traces."""
+def _host_call(p):
+    """pe_forward_host on problem p (host buffers in and out): its traces."""
     import ctypes as C
     from pefdtd import _capi
     from pefdtd.damping import sponge_axis_profiles
     from pefdtd.fdtd import _flat_probe
-    p = make_small(nt=90, shape=(20, 24, 28), n_grains=8, sponge=3)
     shape = p["lab"].shape
     s_idx, s_w, r_off, r_idx, r_w = _flat_probe(shape, p["src_pts"], p["rec_groups"], np.float32)
     cfg = _capi.PeConfig()
@@ -251,8 +251,32 @@ def test_host_entry_matches_device_path():
     out = np.zeros((p["nt"], 1), np.float32)
     _capi.check(_capi.lib().pe_forward_host(C.byref(cfg), _capi.ptr(labs), None, C.byref(md),
                                             C.byref(pr), _capi.ptr(wav), p["nt"], _capi.ptr(out)))
+    return out
+
+
+def test_host_entry_matches_device_path():
+    """pe_forward_host (host buffers in and out) == the oracle's traces."""
+    p = make_small(nt=90, shape=(20, 24, 28), n_grains=8, sponge=3)
+    out = _host_call(p)
     ref = O.run_oracle(oracle_prob(p, record="pressure", damped_record=True), fma_mode=1)
     assert np.array_equal(out, ref)
+
+
+def test_host_entry_reuses_and_releases_its_buffers():
+    """Calls of growing and shrinking sizes reuse the entry's kept buffers
+    and the cache of solver buffers (a larger call grows them; a smaller one
+    takes the same ones, with a zeroed state); every call gives the oracle's
+    traces, before and after the kept memory is released."""
+    from pefdtd import _capi
+    small = make_small(nt=70, shape=(18, 22, 24), n_grains=6, sponge=3, seed=41)
+    large = make_small(nt=90, shape=(26, 30, 36), n_grains=9, sponge=3, seed=42)
+    refs = {id(q): O.run_oracle(oracle_prob(q, record="pressure", damped_record=True), fma_mode=1)
+            for q in (small, large)}
+    for q in (small, large, small, large):
+        assert np.array_equal(_host_call(q), refs[id(q)])
+    _capi.lib().pe_release_cached_memory()
+    for q in (large, small):
+        assert np.array_equal(_host_call(q), refs[id(q)])
 
 
 def test_gpu_labeller_bit_exact():
