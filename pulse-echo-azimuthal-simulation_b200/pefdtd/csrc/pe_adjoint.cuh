@@ -71,14 +71,16 @@ __device__ __forceinline__ float adj_damp(const AdjArgs<T> &A, int iz, int iy, i
 // y + o does not exist reads the operand at y instead (always in the grid)
 // and contributes c * 0, which leaves the sum unchanged bit for bit: every
 // load is independent of the guards, so the gathers of a cell overlap.
-template <typename T, typename F>
+// G: evaluate the guards (false where the caller has established that every
+// tap of the cell exists: adj_block_inside).
+template <typename T, bool G = true, typename F>
 __device__ __forceinline__ T DfT(const F &f, int y, int n, const T c[4], int nc)
 {
     T a = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (j < nc) {
-            const bool p1 = gF(y - j - 1, j, n), p2 = gF(y + j, j, n);
+            const bool p1 = !G || gF(y - j - 1, j, n), p2 = !G || gF(y + j, j, n);
             const T v1 = f(p1 ? -j - 1 : 0), v2 = f(p2 ? j : 0);
             a += c[j] * (p1 ? v1 : T(0));
             a -= c[j] * (p2 ? v2 : T(0));
@@ -86,14 +88,14 @@ __device__ __forceinline__ T DfT(const F &f, int y, int n, const T c[4], int nc)
     }
     return a;
 }
-template <typename T, typename F>
+template <typename T, bool G = true, typename F>
 __device__ __forceinline__ T DbT(const F &f, int y, int n, const T c[4], int nc)
 {
     T a = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (j < nc) {
-            const bool p1 = gB(y - j, j, n), p2 = gB(y + j + 1, j, n);
+            const bool p1 = !G || gB(y - j, j, n), p2 = !G || gB(y + j + 1, j, n);
             const T v1 = f(p1 ? -j : 0), v2 = f(p2 ? j + 1 : 0);
             a += c[j] * (p1 ? v1 : T(0));
             a -= c[j] * (p2 ? v2 : T(0));
@@ -123,6 +125,22 @@ __device__ __forceinline__ bool adj_cell(const AdjArgs<T> &A, long long &i, int 
     iz = blockIdx.z;
     i = ((long long)iz * A.ny + iy) * A.nx + ix;
     return ix < A.nx && iy < A.ny;
+}
+
+// Every cell of this block lies at least ADJ_MARGIN_LO cells from the low
+// faces and ADJ_MARGIN_HI from the high ones. Then every guard of the kernels
+// below holds at every cell of the block: the transposed taps (DfT / DbT:
+// forward cells y - 2j - 1 ... y + 2j + 1 with j <= 3, guards true for
+// 7 <= y <= n - 8), the forward strains (4 <= y <= n - 5) and the moves and
+// their transposes (2 <= y <= n - 3). Such blocks run the unguarded
+// instantiations, whose arithmetic is the guarded one with every guard true.
+constexpr int ADJ_MARGIN_LO = 7, ADJ_MARGIN_HI = 8;
+template <typename T>
+__device__ __forceinline__ bool adj_block_inside(const AdjArgs<T> &A)
+{
+    const int x0 = blockIdx.x * ADJ_BX, y0 = blockIdx.y * ADJ_BY, z = blockIdx.z;
+    return x0 >= ADJ_MARGIN_LO && x0 + ADJ_BX - 1 <= A.nx - ADJ_MARGIN_HI && y0 >= ADJ_MARGIN_LO &&
+           y0 + ADJ_BY - 1 <= A.ny - ADJ_MARGIN_HI && z >= ADJ_MARGIN_LO && z <= A.nz - ADJ_MARGIN_HI;
 }
 
 // ---------------------------------------------------------------- receivers
@@ -183,32 +201,35 @@ __global__ void k_adj_vel_u(AdjArgs<T> A)
     A.u[2][i] = adj_div(s * A.lv[2][i], rvz, r0, A.rinv, m0);
 }
 
+template <typename T, bool G>
+__device__ __forceinline__ void adj_vel_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
+{
+    const long long sy = A.sy, sz = A.sz;
+    const T *ux = A.u[0] + i, *uy = A.u[1] + i, *uz = A.u[2] + i;
+    auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
+    auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
+    auto Z = [&](const T *p) { return [p, sz](int o) { return p[o * sz]; }; };
+    A.ls[0][i] += DfT<T, G>(X(ux), ix, A.nx, A.c, A.nc);
+    A.ls[1][i] += DfT<T, G>(Y(uy), iy, A.ny, A.c, A.nc);
+    A.ls[2][i] += DfT<T, G>(Z(uz), iz, A.nz, A.c, A.nc);
+    A.ls[3][i] += DbT<T, G>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T, G>(Y(uz), iy, A.ny, A.c, A.nc);
+    A.ls[4][i] += DbT<T, G>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T, G>(X(uz), ix, A.nx, A.c, A.nc);
+    A.ls[5][i] += DbT<T, G>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T, G>(X(uy), ix, A.nx, A.c, A.nc);
+}
 template <typename T>
 __global__ void k_adj_vel(AdjArgs<T> A)
 {
     long long i;
     int iz, iy, ix;
     if (!adj_cell(A, i, iz, iy, ix)) return;
-    const long long sy = A.sy, sz = A.sz;
-    const T *ux = A.u[0] + i, *uy = A.u[1] + i, *uz = A.u[2] + i;
-    auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
-    auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
-    auto Z = [&](const T *p) { return [p, sz](int o) { return p[o * sz]; }; };
-    A.ls[0][i] += DfT<T>(X(ux), ix, A.nx, A.c, A.nc);
-    A.ls[1][i] += DfT<T>(Y(uy), iy, A.ny, A.c, A.nc);
-    A.ls[2][i] += DfT<T>(Z(uz), iz, A.nz, A.c, A.nc);
-    A.ls[3][i] += DbT<T>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T>(Y(uz), iy, A.ny, A.c, A.nc);
-    A.ls[4][i] += DbT<T>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T>(X(uz), ix, A.nx, A.c, A.nc);
-    A.ls[5][i] += DbT<T>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T>(X(uy), ix, A.nx, A.c, A.nc);
+    if (adj_block_inside(A)) adj_vel_cell<T, false>(A, i, iz, iy, ix);
+    else adj_vel_cell<T, true>(A, i, iz, iy, ix);
 }
 
 // ---------------------------------------------------------------- strains of v^{n-1}
-template <typename T>
-__global__ void k_adj_strain(AdjArgs<T> A)
+template <typename T, bool G>
+__device__ __forceinline__ void adj_strain_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
-    long long i;
-    int iz, iy, ix;
-    if (!adj_cell(A, i, iz, iy, ix)) return;
     const long long sy = A.sy, sz = A.sz;
     const T *vx = A.vp[0], *vy = A.vp[1], *vz = A.vp[2];
     T a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
@@ -221,8 +242,8 @@ __global__ void k_adj_strain(AdjArgs<T> A)
     for (int j = 0; j < 4; ++j) {
         if (j < A.nc) {
             const T cj = A.c[j];
-            const bool bx = gB(ix, j, A.nx), by = gB(iy, j, A.ny), bz = gB(iz, j, A.nz);
-            const bool fx = gF(ix, j, A.nx), fy = gF(iy, j, A.ny), fz = gF(iz, j, A.nz);
+            const bool bx = !G || gB(ix, j, A.nx), by = !G || gB(iy, j, A.ny), bz = !G || gB(iz, j, A.nz);
+            const bool fx = !G || gF(ix, j, A.nx), fy = !G || gF(iy, j, A.ny), fz = !G || gF(iz, j, A.nz);
             a1 = fmac(a1, cj, d(vx, bx, j, -(j + 1)));
             a2 = fmac(a2, cj, d(vy, by, j * sy, -(j + 1) * sy));
             a3 = fmac(a3, cj, d(vz, bz, j * sz, -(j + 1) * sz));
@@ -237,6 +258,15 @@ __global__ void k_adj_strain(AdjArgs<T> A)
     const T ih = A.inv_h;
     A.g[0][i] = a1 * ih; A.g[1][i] = a2 * ih; A.g[2][i] = a3 * ih;
     A.g[3][i] = a4 * ih; A.g[4][i] = a5 * ih; A.g[5][i] = a6 * ih;
+}
+template <typename T>
+__global__ void k_adj_strain(AdjArgs<T> A)
+{
+    long long i;
+    int iz, iy, ix;
+    if (!adj_cell(A, i, iz, iy, ix)) return;
+    if (adj_block_inside(A)) adj_strain_cell<T, false>(A, i, iz, iy, ix);
+    else adj_strain_cell<T, true>(A, i, iz, iy, ix);
 }
 
 // move guard at forward cell (z, y, x) for offsets d (exactly the forward's)
@@ -294,7 +324,7 @@ static_assert(ADJ_BX == 32, "a warp is one row of an adjoint block");
 // same tap order). The taps are loaded unconditionally, from the cell itself
 // where the move is off the grid, and masked afterwards: no load waits on a
 // guard, so the gathers of a cell are all in flight together.
-template <typename T, int P, int J>
+template <typename T, int P, int J, bool G>
 __device__ __forceinline__ T adj_q(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
     constexpr int S = vpos(J);
@@ -302,7 +332,7 @@ __device__ __forceinline__ T adj_q(const AdjArgs<T> &A, long long i, int iz, int
     if constexpr (DZ == 0 && DY == 0 && DX == 0) {
         return A.g[J][i];
     } else {
-        const bool ok = move_ok(iz, iy, ix, DZ, DY, DX, A.nz, A.ny, A.nx);
+        const bool ok = !G || move_ok(iz, iy, ix, DZ, DY, DX, A.nz, A.ny, A.nx);
         const T *g = A.g[J];
         T acc = 0;
 #pragma unroll
@@ -320,7 +350,7 @@ __device__ __forceinline__ T adj_q(const AdjArgs<T> &A, long long i, int iz, int
 // position of J) or the transposed move of W[P][J] gathered from the forward
 // cells x = i - o of every tap offset o (guards evaluated at x, loads
 // unconditional as in adj_q)
-template <typename T, int J, int P>
+template <typename T, int J, int P, bool G>
 __device__ __forceinline__ void adj_t(const AdjArgs<T> &A, long long i, int iz, int iy, int ix, const T *Cm,
                                       const T (&e)[6], T &acc)
 {
@@ -338,34 +368,75 @@ __device__ __forceinline__ void adj_t(const AdjArgs<T> &A, long long i, int iz, 
             for (int a1 = (DY < 0 ? -1 : 0); a1 <= (DY > 0 ? 1 : 0); ++a1)
 #pragma unroll
                 for (int a2 = (DX < 0 ? -1 : 0); a2 <= (DX > 0 ? 1 : 0); ++a2) {
-                    const bool ok = move_ok(iz - a0, iy - a1, ix - a2, DZ, DY, DX, A.nz, A.ny, A.nx);
+                    const bool ok = !G || move_ok(iz - a0, iy - a1, ix - a2, DZ, DY, DX, A.nz, A.ny, A.nx);
                     const T v = w[ok ? i - a0 * A.sz - a1 * A.sy - a2 : i];
                     acc += T(0.25) * (ok ? v : T(0));
                 }
     }
 }
 
-template <typename T, int J>
+template <typename T, int J, bool G>
 __device__ __forceinline__ T adj_tJ(const AdjArgs<T> &A, long long i, int iz, int iy, int ix, const T *Cm,
                                     const T (&e)[6])
 {
     T acc = 0;
-    adj_t<T, J, 0>(A, i, iz, iy, ix, Cm, e, acc);
-    adj_t<T, J, 1>(A, i, iz, iy, ix, Cm, e, acc);
-    adj_t<T, J, 2>(A, i, iz, iy, ix, Cm, e, acc);
-    adj_t<T, J, 3>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 0, G>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 1, G>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 2, G>(A, i, iz, iy, ix, Cm, e, acc);
+    adj_t<T, J, 3, G>(A, i, iz, iy, ix, Cm, e, acc);
     return acc;
 }
 
-template <typename T, int P>
+template <typename T, int P, bool G>
 __device__ __forceinline__ void adj_qrow(const AdjArgs<T> &A, long long i, int iz, int iy, int ix, T (&q)[6])
 {
-    q[0] = adj_q<T, P, 0>(A, i, iz, iy, ix);
-    q[1] = adj_q<T, P, 1>(A, i, iz, iy, ix);
-    q[2] = adj_q<T, P, 2>(A, i, iz, iy, ix);
-    q[3] = adj_q<T, P, 3>(A, i, iz, iy, ix);
-    q[4] = adj_q<T, P, 4>(A, i, iz, iy, ix);
-    q[5] = adj_q<T, P, 5>(A, i, iz, iy, ix);
+    q[0] = adj_q<T, P, 0, G>(A, i, iz, iy, ix);
+    q[1] = adj_q<T, P, 1, G>(A, i, iz, iy, ix);
+    q[2] = adj_q<T, P, 2, G>(A, i, iz, iy, ix);
+    q[3] = adj_q<T, P, 3, G>(A, i, iz, iy, ix);
+    q[4] = adj_q<T, P, 4, G>(A, i, iz, iy, ix);
+    q[5] = adj_q<T, P, 5, G>(A, i, iz, iy, ix);
+}
+
+// the cell's 21 gradient terms into its row of the warp's reduction tile
+template <typename T, bool G>
+__device__ __forceinline__ bool adj_grad_terms(const AdjArgs<T> &A, long long i, int iz, int iy, int ix,
+                                               const T (&e)[6], double *row)
+{
+    // moved strains at this cell, q[p][J]
+    T q[4][6];
+    adj_qrow<T, 0, G>(A, i, iz, iy, ix, q[0]);
+    adj_qrow<T, 1, G>(A, i, iz, iy, ix, q[1]);
+    adj_qrow<T, 2, G>(A, i, iz, iy, ix, q[2]);
+    adj_qrow<T, 3, G>(A, i, iz, iy, ix, q[3]);
+    // dJ/dC_IJ for I <= J: e_I q[p(I)][J] + e_J q[p(J)][I]  (I != J),
+    // formed in the solve's precision (in FP32 one rounding of the
+    // cell's term, as its fields carry) and summed over cells in f64
+    bool any = false;
+#pragma unroll
+    for (int I = 0; I < 6; ++I)
+#pragma unroll
+        for (int J = I; J < 6; ++J) {
+            T v = e[I] * q[vpos(I)][J];
+            if (J != I) v += e[J] * q[vpos(J)][I];
+            row[c21_slot(I, J)] = (double)v;
+            any = any || v != T(0);
+        }
+    return any;
+}
+
+// strain adjoint t_J: direct term plus transposed moves of
+// W[p][J](x) = sum_{I at p} C_IJ(x) e_I(x) from the forward cells x
+template <typename T, bool G>
+__device__ __forceinline__ void adj_strain_adjoint(const AdjArgs<T> &A, long long i, int iz, int iy, int ix,
+                                                   const T *Cm, const T (&e)[6])
+{
+    A.t[0][i] = adj_tJ<T, 0, G>(A, i, iz, iy, ix, Cm, e);
+    A.t[1][i] = adj_tJ<T, 1, G>(A, i, iz, iy, ix, Cm, e);
+    A.t[2][i] = adj_tJ<T, 2, G>(A, i, iz, iy, ix, Cm, e);
+    A.t[3][i] = adj_tJ<T, 3, G>(A, i, iz, iy, ix, Cm, e);
+    A.t[4][i] = adj_tJ<T, 4, G>(A, i, iz, iy, ix, Cm, e);
+    A.t[5][i] = adj_tJ<T, 5, G>(A, i, iz, iy, ix, Cm, e);
 }
 
 template <typename T>
@@ -391,28 +462,13 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
     int m = -1;
     bool any = false;
     T e[6];
+    const bool inside = adj_block_inside(A);   // block-uniform
     if (live) {
         m = A.lab[i] & LAB_MAT;
 #pragma unroll
         for (int I = 0; I < 6; ++I) e[I] = A.dt * A.ls[I][i];
-        // moved strains at this cell, q[p][J]
-        T q[4][6];
-        adj_qrow<T, 0>(A, i, iz, iy, ix, q[0]);
-        adj_qrow<T, 1>(A, i, iz, iy, ix, q[1]);
-        adj_qrow<T, 2>(A, i, iz, iy, ix, q[2]);
-        adj_qrow<T, 3>(A, i, iz, iy, ix, q[3]);
-        // dJ/dC_IJ for I <= J: e_I q[p(I)][J] + e_J q[p(J)][I]  (I != J),
-        // formed in the solve's precision (in FP32 one rounding of the
-        // cell's term, as its fields carry) and summed over cells in f64
-#pragma unroll
-        for (int I = 0; I < 6; ++I)
-#pragma unroll
-            for (int J = I; J < 6; ++J) {
-                T v = e[I] * q[vpos(I)][J];
-                if (J != I) v += e[J] * q[vpos(J)][I];
-                red[warp][lane][c21_slot(I, J)] = (double)v;
-                any = any || v != T(0);
-            }
+        any = inside ? adj_grad_terms<T, false>(A, i, iz, iy, ix, e, red[warp][lane])
+                     : adj_grad_terms<T, true>(A, i, iz, iy, ix, e, red[warp][lane]);
     } else {
 #pragma unroll
         for (int k = 0; k < 21; ++k) red[warp][lane][k] = 0.0;
@@ -444,15 +500,9 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
         }
     }
     if (!live) return;
-    // strain adjoint t_J: direct term plus transposed moves of
-    // W[p][J](x) = sum_{I at p} C_IJ(x) e_I(x) from the forward cells x
     const T *Cm = A.c21 + (long long)m * C21_STRIDE;
-    A.t[0][i] = adj_tJ<T, 0>(A, i, iz, iy, ix, Cm, e);
-    A.t[1][i] = adj_tJ<T, 1>(A, i, iz, iy, ix, Cm, e);
-    A.t[2][i] = adj_tJ<T, 2>(A, i, iz, iy, ix, Cm, e);
-    A.t[3][i] = adj_tJ<T, 3>(A, i, iz, iy, ix, Cm, e);
-    A.t[4][i] = adj_tJ<T, 4>(A, i, iz, iy, ix, Cm, e);
-    A.t[5][i] = adj_tJ<T, 5>(A, i, iz, iy, ix, Cm, e);
+    if (inside) adj_strain_adjoint<T, false>(A, i, iz, iy, ix, Cm, e);
+    else adj_strain_adjoint<T, true>(A, i, iz, iy, ix, Cm, e);
     // the step's last use of ls at this cell (k_adj_w ran before, and only
     // this thread reads it here): apply the deferred damping, ls = d ls (the
     // transpose of the forward s^{n-1} * d)
@@ -474,12 +524,9 @@ __global__ void k_grad_fold(double *rep, int nrep, long long len, double *grad)
     grad[i] += s;
 }
 
-template <typename T>
-__global__ void k_adj_velfin(AdjArgs<T> A)
+template <typename T, bool G>
+__device__ __forceinline__ void adj_velfin_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
-    long long i;
-    int iz, iy, ix;
-    if (!adj_cell(A, i, iz, iy, ix)) return;
     const long long sy = A.sy, sz = A.sz;
     auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
     auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
@@ -488,15 +535,24 @@ __global__ void k_adj_velfin(AdjArgs<T> A)
     const T *t4 = A.t[3] + i, *t5 = A.t[4] + i, *t6 = A.t[5] + i;
     const T d = (T)adj_damp(A, iz, iy, ix, i);
     const T ih = A.inv_h;
-    const T gx = DbT<T>(X(t1), ix, A.nx, A.c, A.nc) + DfT<T>(Z(t5), iz, A.nz, A.c, A.nc) +
-                 DfT<T>(Y(t6), iy, A.ny, A.c, A.nc);
-    const T gy = DbT<T>(Y(t2), iy, A.ny, A.c, A.nc) + DfT<T>(Z(t4), iz, A.nz, A.c, A.nc) +
-                 DfT<T>(X(t6), ix, A.nx, A.c, A.nc);
-    const T gz = DbT<T>(Z(t3), iz, A.nz, A.c, A.nc) + DfT<T>(Y(t4), iy, A.ny, A.c, A.nc) +
-                 DfT<T>(X(t5), ix, A.nx, A.c, A.nc);
+    const T gx = DbT<T, G>(X(t1), ix, A.nx, A.c, A.nc) + DfT<T, G>(Z(t5), iz, A.nz, A.c, A.nc) +
+                 DfT<T, G>(Y(t6), iy, A.ny, A.c, A.nc);
+    const T gy = DbT<T, G>(Y(t2), iy, A.ny, A.c, A.nc) + DfT<T, G>(Z(t4), iz, A.nz, A.c, A.nc) +
+                 DfT<T, G>(X(t6), ix, A.nx, A.c, A.nc);
+    const T gz = DbT<T, G>(Z(t3), iz, A.nz, A.c, A.nc) + DfT<T, G>(Y(t4), iy, A.ny, A.c, A.nc) +
+                 DfT<T, G>(X(t5), ix, A.nx, A.c, A.nc);
     A.lv[0][i] = d * A.lv[0][i] + ih * gx;
     A.lv[1][i] = d * A.lv[1][i] + ih * gy;
     A.lv[2][i] = d * A.lv[2][i] + ih * gz;
+}
+template <typename T>
+__global__ void k_adj_velfin(AdjArgs<T> A)
+{
+    long long i;
+    int iz, iy, ix;
+    if (!adj_cell(A, i, iz, iy, ix)) return;
+    if (adj_block_inside(A)) adj_velfin_cell<T, false>(A, i, iz, iy, ix);
+    else adj_velfin_cell<T, true>(A, i, iz, iy, ix);
 }
 
 }  // namespace pe
