@@ -72,7 +72,8 @@ __device__ __forceinline__ float adj_damp(const AdjArgs<T> &A, int iz, int iy, i
 // and contributes c * 0, which leaves the sum unchanged bit for bit: every
 // load is independent of the guards, so the gathers of a cell overlap.
 // G: evaluate the guards (false where the caller has established that every
-// tap of the cell exists: adj_block_inside).
+// tap of the cell along this axis exists: adj_block_inside, adj_inside_x,
+// adj_inside_yz).
 template <typename T, bool G = true, typename F>
 __device__ __forceinline__ T DfT(const F &f, int y, int n, const T c[4], int nc)
 {
@@ -143,6 +144,33 @@ __device__ __forceinline__ bool adj_block_inside(const AdjArgs<T> &A)
            y0 + ADJ_BY - 1 <= A.ny - ADJ_MARGIN_HI && z >= ADJ_MARGIN_LO && z <= A.nz - ADJ_MARGIN_HI;
 }
 
+// The same test split by axis, for k_adj_strain and k_adj_velfin: a block inside
+// along x (adj_inside_x) runs with the x guards compiled out (GX = false), a
+// block inside along y and z (adj_inside_yz) with the y / z guards compiled
+// out (GYZ = false); most blocks that miss the margins do so along one axis.
+template <typename T>
+__device__ __forceinline__ bool adj_inside_x(const AdjArgs<T> &A)
+{
+    const int x0 = blockIdx.x * ADJ_BX;
+    return x0 >= ADJ_MARGIN_LO && x0 + ADJ_BX - 1 <= A.nx - ADJ_MARGIN_HI;
+}
+template <typename T>
+__device__ __forceinline__ bool adj_inside_yz(const AdjArgs<T> &A)
+{
+    const int y0 = blockIdx.y * ADJ_BY, z = blockIdx.z;
+    return y0 >= ADJ_MARGIN_LO && y0 + ADJ_BY - 1 <= A.ny - ADJ_MARGIN_HI && z >= ADJ_MARGIN_LO &&
+           z <= A.nz - ADJ_MARGIN_HI;
+}
+// f<T, GX, GYZ>(args...) for this block's classification (block-uniform)
+#define ADJ_DISPATCH(A, f, ...)                                          \
+    do {                                                                 \
+        const bool in_x_ = adj_inside_x(A), in_yz_ = adj_inside_yz(A);   \
+        if (in_x_ && in_yz_) f<T, false, false>(__VA_ARGS__);            \
+        else if (in_x_) f<T, false, true>(__VA_ARGS__);                  \
+        else if (in_yz_) f<T, true, false>(__VA_ARGS__);                 \
+        else f<T, true, true>(__VA_ARGS__);                              \
+    } while (0)
+
 // ---------------------------------------------------------------- receivers
 // entries: cells[k] sorted, pos[k] = caller position; w and grp in caller order
 template <typename T>
@@ -201,7 +229,7 @@ __global__ void k_adj_vel_u(AdjArgs<T> A)
     A.u[2][i] = adj_div(s * A.lv[2][i], rvz, r0, A.rinv, m0);
 }
 
-template <typename T, bool G>
+template <typename T, bool GX, bool GYZ>
 __device__ __forceinline__ void adj_vel_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
     const long long sy = A.sy, sz = A.sz;
@@ -209,12 +237,12 @@ __device__ __forceinline__ void adj_vel_cell(const AdjArgs<T> &A, long long i, i
     auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
     auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
     auto Z = [&](const T *p) { return [p, sz](int o) { return p[o * sz]; }; };
-    A.ls[0][i] += DfT<T, G>(X(ux), ix, A.nx, A.c, A.nc);
-    A.ls[1][i] += DfT<T, G>(Y(uy), iy, A.ny, A.c, A.nc);
-    A.ls[2][i] += DfT<T, G>(Z(uz), iz, A.nz, A.c, A.nc);
-    A.ls[3][i] += DbT<T, G>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T, G>(Y(uz), iy, A.ny, A.c, A.nc);
-    A.ls[4][i] += DbT<T, G>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T, G>(X(uz), ix, A.nx, A.c, A.nc);
-    A.ls[5][i] += DbT<T, G>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T, G>(X(uy), ix, A.nx, A.c, A.nc);
+    A.ls[0][i] += DfT<T, GX>(X(ux), ix, A.nx, A.c, A.nc);
+    A.ls[1][i] += DfT<T, GYZ>(Y(uy), iy, A.ny, A.c, A.nc);
+    A.ls[2][i] += DfT<T, GYZ>(Z(uz), iz, A.nz, A.c, A.nc);
+    A.ls[3][i] += DbT<T, GYZ>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T, GYZ>(Y(uz), iy, A.ny, A.c, A.nc);
+    A.ls[4][i] += DbT<T, GYZ>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T, GX>(X(uz), ix, A.nx, A.c, A.nc);
+    A.ls[5][i] += DbT<T, GYZ>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T, GX>(X(uy), ix, A.nx, A.c, A.nc);
 }
 template <typename T>
 __global__ void k_adj_vel(AdjArgs<T> A)
@@ -222,12 +250,14 @@ __global__ void k_adj_vel(AdjArgs<T> A)
     long long i;
     int iz, iy, ix;
     if (!adj_cell(A, i, iz, iy, ix)) return;
-    if (adj_block_inside(A)) adj_vel_cell<T, false>(A, i, iz, iy, ix);
-    else adj_vel_cell<T, true>(A, i, iz, iy, ix);
+    // two instantiations (all guards or none): the four of ADJ_DISPATCH
+    // measured slower here (more registers)
+    if (adj_inside_x(A) && adj_inside_yz(A)) adj_vel_cell<T, false, false>(A, i, iz, iy, ix);
+    else adj_vel_cell<T, true, true>(A, i, iz, iy, ix);
 }
 
 // ---------------------------------------------------------------- strains of v^{n-1}
-template <typename T, bool G>
+template <typename T, bool GX, bool GYZ>
 __device__ __forceinline__ void adj_strain_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
     const long long sy = A.sy, sz = A.sz;
@@ -242,8 +272,8 @@ __device__ __forceinline__ void adj_strain_cell(const AdjArgs<T> &A, long long i
     for (int j = 0; j < 4; ++j) {
         if (j < A.nc) {
             const T cj = A.c[j];
-            const bool bx = !G || gB(ix, j, A.nx), by = !G || gB(iy, j, A.ny), bz = !G || gB(iz, j, A.nz);
-            const bool fx = !G || gF(ix, j, A.nx), fy = !G || gF(iy, j, A.ny), fz = !G || gF(iz, j, A.nz);
+            const bool bx = !GX || gB(ix, j, A.nx), by = !GYZ || gB(iy, j, A.ny), bz = !GYZ || gB(iz, j, A.nz);
+            const bool fx = !GX || gF(ix, j, A.nx), fy = !GYZ || gF(iy, j, A.ny), fz = !GYZ || gF(iz, j, A.nz);
             a1 = fmac(a1, cj, d(vx, bx, j, -(j + 1)));
             a2 = fmac(a2, cj, d(vy, by, j * sy, -(j + 1) * sy));
             a3 = fmac(a3, cj, d(vz, bz, j * sz, -(j + 1) * sz));
@@ -265,8 +295,7 @@ __global__ void k_adj_strain(AdjArgs<T> A)
     long long i;
     int iz, iy, ix;
     if (!adj_cell(A, i, iz, iy, ix)) return;
-    if (adj_block_inside(A)) adj_strain_cell<T, false>(A, i, iz, iy, ix);
-    else adj_strain_cell<T, true>(A, i, iz, iy, ix);
+    ADJ_DISPATCH(A, adj_strain_cell, A, i, iz, iy, ix);
 }
 
 // move guard at forward cell (z, y, x) for offsets d (exactly the forward's)
@@ -524,7 +553,7 @@ __global__ void k_grad_fold(double *rep, int nrep, long long len, double *grad)
     grad[i] += s;
 }
 
-template <typename T, bool G>
+template <typename T, bool GX, bool GYZ>
 __device__ __forceinline__ void adj_velfin_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
     const long long sy = A.sy, sz = A.sz;
@@ -535,12 +564,12 @@ __device__ __forceinline__ void adj_velfin_cell(const AdjArgs<T> &A, long long i
     const T *t4 = A.t[3] + i, *t5 = A.t[4] + i, *t6 = A.t[5] + i;
     const T d = (T)adj_damp(A, iz, iy, ix, i);
     const T ih = A.inv_h;
-    const T gx = DbT<T, G>(X(t1), ix, A.nx, A.c, A.nc) + DfT<T, G>(Z(t5), iz, A.nz, A.c, A.nc) +
-                 DfT<T, G>(Y(t6), iy, A.ny, A.c, A.nc);
-    const T gy = DbT<T, G>(Y(t2), iy, A.ny, A.c, A.nc) + DfT<T, G>(Z(t4), iz, A.nz, A.c, A.nc) +
-                 DfT<T, G>(X(t6), ix, A.nx, A.c, A.nc);
-    const T gz = DbT<T, G>(Z(t3), iz, A.nz, A.c, A.nc) + DfT<T, G>(Y(t4), iy, A.ny, A.c, A.nc) +
-                 DfT<T, G>(X(t5), ix, A.nx, A.c, A.nc);
+    const T gx = DbT<T, GX>(X(t1), ix, A.nx, A.c, A.nc) + DfT<T, GYZ>(Z(t5), iz, A.nz, A.c, A.nc) +
+                 DfT<T, GYZ>(Y(t6), iy, A.ny, A.c, A.nc);
+    const T gy = DbT<T, GYZ>(Y(t2), iy, A.ny, A.c, A.nc) + DfT<T, GYZ>(Z(t4), iz, A.nz, A.c, A.nc) +
+                 DfT<T, GX>(X(t6), ix, A.nx, A.c, A.nc);
+    const T gz = DbT<T, GYZ>(Z(t3), iz, A.nz, A.c, A.nc) + DfT<T, GYZ>(Y(t4), iy, A.ny, A.c, A.nc) +
+                 DfT<T, GX>(X(t5), ix, A.nx, A.c, A.nc);
     A.lv[0][i] = d * A.lv[0][i] + ih * gx;
     A.lv[1][i] = d * A.lv[1][i] + ih * gy;
     A.lv[2][i] = d * A.lv[2][i] + ih * gz;
@@ -551,8 +580,7 @@ __global__ void k_adj_velfin(AdjArgs<T> A)
     long long i;
     int iz, iy, ix;
     if (!adj_cell(A, i, iz, iy, ix)) return;
-    if (adj_block_inside(A)) adj_velfin_cell<T, false>(A, i, iz, iy, ix);
-    else adj_velfin_cell<T, true>(A, i, iz, iy, ix);
+    ADJ_DISPATCH(A, adj_velfin_cell, A, i, iz, iy, ix);
 }
 
 }  // namespace pe
