@@ -430,7 +430,7 @@ __device__ __forceinline__ void adj_qrow(const AdjArgs<T> &A, long long i, int i
 // the cell's 21 gradient terms into its row of the warp's reduction tile
 template <typename T, bool G>
 __device__ __forceinline__ bool adj_grad_terms(const AdjArgs<T> &A, long long i, int iz, int iy, int ix,
-                                               const T (&e)[6], double *row)
+                                               const T (&e)[6], T *row)
 {
     // moved strains at this cell, q[p][J]
     T q[4][6];
@@ -448,7 +448,7 @@ __device__ __forceinline__ bool adj_grad_terms(const AdjArgs<T> &A, long long i,
         for (int J = I; J < 6; ++J) {
             T v = e[I] * q[vpos(I)][J];
             if (J != I) v += e[J] * q[vpos(J)][I];
-            row[c21_slot(I, J)] = (double)v;
+            row[c21_slot(I, J)] = v;
             any = any || v != T(0);
         }
     return any;
@@ -482,9 +482,13 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
     // formed keeps them out of registers during the gathers that follow.
     // Warps add into one of grad_rep replicas of the table (by warp index),
     // so that the warps of a large single-material region (the couplant) do
-    // not all serialise on the same 21 addresses. Tile rows are 21 doubles
-    // apart: row stores and column loads are free of bank conflicts.
-    __shared__ double red[ADJ_STRESS_WARPS][32][21];
+    // not all serialise on the same 21 addresses. The tile holds the terms in
+    // the solve's precision (each is one rounding in T) and the column sums
+    // convert them to f64 as they add them, exactly: in FP32 this halves the
+    // tile (21.5 KB per block) and leaves that much more of the SM's unified
+    // L1 to the gathers. Tile rows are 21 elements apart (odd): row stores and
+    // column loads are free of bank conflicts.
+    __shared__ T red[ADJ_STRESS_WARPS][32][21];
     __shared__ int rmat[ADJ_STRESS_WARPS][32];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.y;
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
                      : adj_grad_terms<T, true>(A, i, iz, iy, ix, e, red[warp][lane]);
     } else {
 #pragma unroll
-        for (int k = 0; k < 21; ++k) red[warp][lane][k] = 0.0;
+        for (int k = 0; k < 21; ++k) red[warp][lane][k] = T(0);
     }
     rmat[warp][lane] = m;
     __syncwarp();
@@ -520,10 +524,10 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
             double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;   // four chains, for latency
 #pragma unroll
             for (int r = 0; r < 32; r += 4) {
-                v0 += rmat[warp][r] == mm ? red[warp][r][lane] : 0.0;
-                v1 += rmat[warp][r + 1] == mm ? red[warp][r + 1][lane] : 0.0;
-                v2 += rmat[warp][r + 2] == mm ? red[warp][r + 2][lane] : 0.0;
-                v3 += rmat[warp][r + 3] == mm ? red[warp][r + 3][lane] : 0.0;
+                v0 += rmat[warp][r] == mm ? (double)red[warp][r][lane] : 0.0;
+                v1 += rmat[warp][r + 1] == mm ? (double)red[warp][r + 1][lane] : 0.0;
+                v2 += rmat[warp][r + 2] == mm ? (double)red[warp][r + 2][lane] : 0.0;
+                v3 += rmat[warp][r + 3] == mm ? (double)red[warp][r + 3][lane] : 0.0;
             }
             atomicAdd(gtab + (long long)mm * 21 + lane, (v0 + v1) + (v2 + v3));
         }
