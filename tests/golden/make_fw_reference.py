@@ -12,6 +12,15 @@ fluid damping 0.02, a rim probe 6.35 mm across. Its gate
 (sim/core/validate_labels.py:103-132): correlation > 0.999 and coda level
 within 0.2 dB.
 
+The six azimuth traces sim/ref/fw_az{17,31,47,62,76,90}.npz
+(sim/pipeline/azimuth_sweep.py:62-120: the same specimen resampled by
+`rotation_test.rotated_grid`, dt from `safe_dt_labels` per azimuth) are
+stored too, with the digests of the rotated grids and the c-axes in both
+rotation conventions: `axes @ R` (the reference's current `rotated_grid`,
+sim/core/rotation_test.py:66-75, 132-134) and `axes @ R.T`, the convention
+that code replaced, which the stored azimuth traces were computed with (they
+are dated before the fix, azimuth_sweep.py:18).
+
 Stored here: the four traces with their dt, E1 and level, the four fabric
 axis sets, and a digest of the solver grid built by this repository's
 `specimen.DiskSpecimen(...).build(h, labeller="exact")` + `build_grid` (the
@@ -36,6 +45,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 OUT = os.path.join(HERE, "fw_reference_2mhz.npz")
 TAGS = ("00", "25", "50", "100")
+AZIMUTHS = (17, 31, 47, 62, 76, 90)
 SPEC = dict(diameter_m=0.100, thickness_m=0.035, n_grains=100, size_cv=0.35, concentration=3.93,
             spatial_corr=0.0, fabric_axis=(1, 0, 0), seed=7)
 H = 3850.0 / 2e6 / 6.0
@@ -79,10 +89,33 @@ def main():
         lvl.append(float(d["level_db"]))
         frac.append(float(d["frac"]))
     assert len({len(t) for t in traces}) == 1 and len(set(dts)) == 1
+    from rotation_test import rotated_grid as ref_rotated_grid   # the reference's
+    az_rot, az_tr, az_dt, az_lvl, az_dig, az_cur, az_leg = [], [], [], [], [], [], []
+    for rot in AZIMUTHS:
+        d = np.load(os.path.join(ref, "sim", "ref", f"fw_az{rot:02d}.npz"))
+        assert float(d["fluid_damp"]) == 0.02 and int(d["rot_deg"]) == rot
+        rl, rnd, rm, rax = ref_rotated_grid(dict(labels=ours["labels"], axes=ours["axes"], h=H), H, SPONGE, rot)
+        ol, ond, om, oax = specimen.rotated_grid(ours["labels"], ours["axes"], H, H, SPONGE, rot)
+        assert np.array_equal(rl, ol) and np.array_equal(rax, oax) and (rnd, rm) == (ond, om)
+        a = np.radians(rot)
+        R = np.array([[np.cos(a), -np.sin(a), 0.0], [np.sin(a), np.cos(a), 0.0], [0.0, 0.0, 1.0]])
+        az_rot.append(rot)
+        az_tr.append(np.asarray(d["trace"], np.float64).ravel())
+        az_dt.append(float(d["dt"]))
+        az_lvl.append(float(d["level_db"]))
+        az_dig.append(grid_digest(ol))
+        az_cur.append(oax)
+        az_leg.append(ours["axes"] @ R.T)
+    az_len = np.array([len(t) for t in az_tr])      # nt differs with dt per azimuth
+    az_pad = np.zeros((len(az_tr), int(az_len.max())))
+    for i, t in enumerate(az_tr):
+        az_pad[i, :len(t)] = t
     np.savez_compressed(OUT, traces=np.stack(traces), dt=dts[0], E1=np.array(e1), level_db=np.array(lvl),
                         frac=np.array(frac), axes=fabrics, h=H, sponge=SPONGE, fluid_damp=0.02, f0=2e6,
                         grid_shape=np.array(lab.shape), nd=nd, m=m, grid_digest=grid_digest(lab),
-                        labeller_cells_differing=n_diff)
+                        labeller_cells_differing=n_diff, az_rot=np.array(az_rot), az_traces=az_pad, az_len=az_len,
+                        az_dt=np.array(az_dt), az_level_db=np.array(az_lvl), az_grid_digest=np.array(az_dig),
+                        az_axes_current=np.stack(az_cur), az_axes_legacy=np.stack(az_leg))
     print(f"wrote {OUT}: grid {lab.shape}, {len(traces[0])} samples, dt {dts[0]:.6e}", flush=True)
 
 

@@ -16,7 +16,15 @@ and damping) land 2.2-2.4 % (relative L2) from every stored trace, from the
 direct pulse on, exactly where this solver lands. So the tests are: the
 reference's gate on fabric 0; this solver against the reference's current
 kernels on all four fabrics; and every stored trace matched at the
-correlation bound, at the same distance as the reference's own kernels."""
+correlation bound, at the same distance as the reference's own kernels.
+
+sim/ref/fw_az{17,...,90}.npz hold the same specimen rotated about the disc
+axis (sim/pipeline/azimuth_sweep.py:62-120). They were computed before the
+reference changed the c-axis rotation of `rotated_grid` from `axes @ R.T` to
+`axes @ R` (sim/core/rotation_test.py:66-75): with the old convention this
+solver matches them at correlation 0.9995, with the current one it does not
+(the coda levels differ by 8-11 dB). The azimuth tests use the old
+convention on the grid `rotated_grid` builds."""
 import os
 
 import numpy as np
@@ -53,6 +61,25 @@ def rim_probe(lab, nd, h):
             if dy * dy + dz * dz <= er * er and lab[cz + dz, cy + dy, ixp] >= 0]
 
 
+def clean_level(x, dt):
+    """dB of the envelope RMS in 24-36 us against E1, the azimuth traces'
+    level (sim/pipeline/azimuth_sweep.py:94-100, ladder.W_CLEAN)."""
+    from scipy.signal import hilbert
+    e = np.abs(hilbert(x))
+    k0 = int(2 * 0.100 / C_REF / dt)
+    E1 = e[max(k0 - int(2e-6 / dt), 0):k0 + int(2e-6 / dt)].max()
+    w = e[int(24e-6 / dt):int(36e-6 / dt)]
+    return 20 * np.log10(np.sqrt((w ** 2).mean()) / E1 + 1e-30)
+
+
+def test_azimuth_metric_reproduces_the_stored_levels():
+    """CPU: each stored azimuth trace's recorded level is clean_level of it."""
+    g = np.load(GOLD)
+    for k in range(len(g["az_rot"])):
+        tr = g["az_traces"][k, :int(g["az_len"][k])]
+        assert abs(clean_level(tr, float(g["az_dt"][k])) - float(g["az_level_db"][k])) < 1e-9
+
+
 def test_gate_metric_reproduces_the_stored_levels():
     """CPU: the gate's coda metric, restated here, gives each stored trace's
     own recorded level (fw_reference_2mhz.py computed it with the same
@@ -75,29 +102,30 @@ def ladder_case():
     assert hashlib.sha256(np.ascontiguousarray(lab, np.int32).tobytes()).hexdigest() == str(g["grid_digest"])
     dm = damping.fluid_damp_mask(lab, float(g["fluid_damp"]))
     pts = rim_probe(lab, nd, h)
-    return dict(g=g, lab=lab, h=h, sponge=sponge, dm=dm, pts=pts, co=coeffs.optimised_coeffs(8))
+    return dict(g=g, lab=lab, h=h, sponge=sponge, dm=dm, pts=pts, co=coeffs.optimised_coeffs(8), build=build)
 
 
-def _solve(c, k):
+def _solve(c, k, axes=None, dt=None, nt=None):
     from pefdtd import fdtd, wavelets
     g = c["g"]
-    dt, nt = float(g["dt"]), int(g["traces"].shape[1])
+    dt = float(g["dt"]) if dt is None else dt
+    nt = int(g["traces"].shape[1]) if nt is None else nt
+    axes = g["axes"][k] if axes is None else axes
     w = 1.0 / len(c["pts"])
     wav = wavelets.ricker(float(g["f0"]), dt, nt)
     src = [(p, w) for p in c["pts"]]
     rec = [(c["pts"], np.full(len(c["pts"]), w))]
-    tr = np.asarray(fdtd.forward_fused_labels(c["lab"], g["axes"][k], c["h"], dt, nt, src, wav, rec, order=8,
+    tr = np.asarray(fdtd.forward_fused_labels(c["lab"], axes, c["h"], dt, nt, src, wav, rec, order=8,
                                               coeffs=c["co"], sponge_width=c["sponge"], damp_mask=c["dm"]),
                     float).ravel()
-    return tr, dict(src=src, rec=rec, wav=wav, dt=dt, nt=nt)
+    return tr, dict(src=src, rec=rec, wav=wav, dt=dt, nt=nt, axes=axes)
 
 
 def _reference_kernels(c, k, run):
     """The same solve through the reference's own label kernels on the GPU."""
     from oracle import oracle as O
     from pefdtd.materials import material_tables
-    g = c["g"]
-    Ct, rho_t = material_tables(g["axes"][k])
+    Ct, rho_t = material_tables(run["axes"])
     p = dict(lab=c["lab"], mats=c["lab"] + 1, Ct=Ct, rho_t=rho_t, sponge=c["sponge"], src_pts=run["src"],
              rec_groups=run["rec"], h=c["h"], dt=run["dt"], coeffs=c["co"], wavelet=run["wav"], nt=run["nt"],
              record="pressure")
@@ -138,3 +166,30 @@ def test_every_fabric_matches_the_reference_kernels(ladder_case, k):
     assert float(np.corrcoef(tr, stored)[0, 1]) > 0.999
     assert abs(_rel(tr, stored) - _rel(ref, stored)) < 1e-4, (_rel(tr, stored), _rel(ref, stored))
     assert _rel(tr, stored) < 0.03
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rot", [17, 76])
+def test_azimuth_traces_with_the_rotation_they_were_made_with(ladder_case, rot):
+    """The specimen rotated by rot degrees (`rotated_grid`: the grid's
+    digest, and its c-axes those of the reference's current code): with the
+    c-axes rotated as the stored traces were (axes @ R.T), within 1e-5 of the
+    reference's current kernels on the same inputs and correlated > 0.999
+    with the stored trace (76 degrees is the reference's beam walk-off
+    outlier: coda level -22 dB against -45 and -53 dB at 62 and 90)."""
+    import hashlib
+    from pefdtd import damping, specimen
+    c = ladder_case
+    g = c["g"]
+    k = list(g["az_rot"]).index(rot)
+    b = c["build"]
+    lab, nd, m, axr = specimen.rotated_grid(b["labels"], b["axes"], c["h"], c["h"], c["sponge"], rot)
+    assert hashlib.sha256(np.ascontiguousarray(lab, np.int32).tobytes()).hexdigest() == str(g["az_grid_digest"][k])
+    assert np.array_equal(axr, g["az_axes_current"][k])
+    cr = dict(c, lab=lab, dm=damping.fluid_damp_mask(lab, float(g["fluid_damp"])), pts=rim_probe(lab, nd, c["h"]))
+    stored = g["az_traces"][k, :int(g["az_len"][k])]
+    tr, run = _solve(cr, k, axes=g["az_axes_legacy"][k], dt=float(g["az_dt"][k]), nt=len(stored))
+    ref = _reference_kernels(cr, k, run)
+    assert _rel(tr, ref) <= 1e-5, _rel(tr, ref)
+    assert float(np.corrcoef(tr, stored)[0, 1]) > 0.999
+    assert abs(_rel(tr, stored) - _rel(ref, stored)) < 1e-4
