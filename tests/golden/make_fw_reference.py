@@ -1,4 +1,4 @@
-"""Generate tests/golden/fw_reference_2mhz.npz: the reference's own stored
+"""Generate tests/golden/fw_reference.npz: the reference's own stored
 full-wave traces of its ladder specimen with what a GPU test needs to
 recompute them with this solver and apply the reference's acceptance gate.
 
@@ -20,6 +20,12 @@ rotation conventions: `axes @ R` (the reference's current `rotated_grid`,
 sim/core/rotation_test.py:66-75, 132-134) and `axes @ R.T`, the convention
 that code replaced, which the stored azimuth traces were computed with (they
 are dated before the fix, azimuth_sweep.py:18).
+
+Two traces of the same specimen at the probe's higher frequencies are stored
+as well: sim/ref/fw_3mhz.npz (sim/fw_checks/freq_blips.py:170-207, 46 M
+cells, 5937 steps) and sim/ref/fw_5mhz_fabric00.npz
+(sim/fw_checks/fw_reference_5mhz.py:33-80, 194 M cells, 9895 steps), each
+with the digest and c-axes of this repository's build at its spacing.
 
 Stored here: the four traces with their dt, E1 and level, the four fabric
 axis sets, and a digest of the solver grid built by this repository's
@@ -43,7 +49,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-OUT = os.path.join(HERE, "fw_reference_2mhz.npz")
+OUT = os.path.join(HERE, "fw_reference.npz")
 TAGS = ("00", "25", "50", "100")
 AZIMUTHS = (17, 31, 47, 62, 76, 90)
 SPEC = dict(diameter_m=0.100, thickness_m=0.035, n_grains=100, size_cv=0.35, concentration=3.93,
@@ -110,7 +116,24 @@ def main():
     az_pad = np.zeros((len(az_tr), int(az_len.max())))
     for i, t in enumerate(az_tr):
         az_pad[i, :len(t)] = t
-    np.savez_compressed(OUT, traces=np.stack(traces), dt=dts[0], E1=np.array(e1), level_db=np.array(lvl),
+    hf = {}
+    for tag, f0 in (("fw_3mhz", 3e6), ("fw_5mhz_fabric00", 5e6)):
+        d = np.load(os.path.join(ref, "sim", "ref", f"{tag}.npz"))
+        hh = float(d["h"])
+        assert abs(hh - 3850.0 / f0 / 6.0) < 1e-15 and int(d["order"]) == 8 and int(d["seed_specimen"]) == 7
+        t0 = time.time()
+        bh = sp.build(hh, labeller="exact")
+        gl, _, _ = specimen.build_grid(bh["labels"], hh, hh, SPONGE)
+        print(f"{tag}: grid {gl.shape}, {time.time() - t0:.0f} s", flush=True)
+        key = "f3" if f0 == 3e6 else "f5"
+        hf[f"{key}_trace"] = np.asarray(d["trace"], np.float64).ravel()
+        hf[f"{key}_dt"] = float(d["dt"])
+        hf[f"{key}_h"] = hh
+        hf[f"{key}_f0"] = f0
+        hf[f"{key}_axes"] = bh["axes"]
+        hf[f"{key}_grid_digest"] = grid_digest(gl)
+        del bh, gl
+    np.savez_compressed(OUT, **hf, traces=np.stack(traces), dt=dts[0], E1=np.array(e1), level_db=np.array(lvl),
                         frac=np.array(frac), axes=fabrics, h=H, sponge=SPONGE, fluid_damp=0.02, f0=2e6,
                         grid_shape=np.array(lab.shape), nd=nd, m=m, grid_digest=grid_digest(lab),
                         labeller_cells_differing=n_diff, az_rot=np.array(az_rot), az_traces=az_pad, az_len=az_len,
