@@ -25,7 +25,10 @@ Two traces of the same specimen at the probe's higher frequencies are stored
 as well: sim/ref/fw_3mhz.npz (sim/fw_checks/freq_blips.py:170-207, 46 M
 cells, 5937 steps) and sim/ref/fw_5mhz_fabric00.npz
 (sim/fw_checks/fw_reference_5mhz.py:33-80, 194 M cells, 9895 steps), each
-with the digest and c-axes of this repository's build at its spacing.
+with the digest and c-axes of this repository's build at its spacing, and
+the 5 MHz run cropped to the E1 corridor |y| <= 27 mm about the beam axis
+(sim/ref/fw_5mhz_e1corridor.npz, sim/fw_checks/fw_e1_corridor_validate.py:
+49-104).
 
 Stored here: the four traces with their dt, E1 and level, the four fabric
 axis sets, and a digest of the solver grid built by this repository's
@@ -133,6 +136,10 @@ def main():
         hf[f"{key}_axes"] = bh["axes"]
         hf[f"{key}_grid_digest"] = grid_digest(gl)
         del bh, gl
+    d = np.load(os.path.join(ref, "sim", "ref", "fw_5mhz_e1corridor.npz"))
+    assert abs(float(d["dt"]) - hf["f5_dt"]) < 1e-20
+    hf["f5c_trace"] = np.asarray(d["trace"], np.float64).ravel()
+    hf["f5c_half_w"] = float(d["half_w"])
     np.savez_compressed(OUT, **hf, traces=np.stack(traces), dt=dts[0], E1=np.array(e1), level_db=np.array(lvl),
                         frac=np.array(frac), axes=fabrics, h=H, sponge=SPONGE, fluid_damp=0.02, f0=2e6,
                         grid_shape=np.array(lab.shape), nd=nd, m=m, grid_digest=grid_digest(lab),

@@ -28,8 +28,10 @@ convention on the grid `rotated_grid` builds.
 
 sim/ref/fw_3mhz.npz and fw_5mhz_fabric00.npz hold the same specimen at 3 and
 5 MHz (46 M and 194 M cells). They sit at the same 2.2-2.4 % from this
-solver as the 2 MHz set; the 5 MHz solve takes about two minutes of GPU
-time, so its test runs only with PE_LONG_TESTS set."""
+solver as the 2 MHz set. fw_5mhz_e1corridor.npz is the 5 MHz run cropped to
+the E1 corridor |y| <= 27 mm (sim/fw_checks/fw_e1_corridor_validate.py),
+recomputed with crop.e1_corridor. The 5 MHz solves take about four minutes
+of GPU time together, so their test runs only with PE_LONG_TESTS set."""
 import os
 
 import numpy as np
@@ -200,6 +202,34 @@ def test_azimuth_traces_with_the_rotation_they_were_made_with(ladder_case, rot):
     assert abs(_rel(tr, stored) - _rel(ref, stored)) < 1e-4
 
 
+def e1_of(x, dt):
+    """(E1, its time): the envelope maximum within 2 us of the 2 x 100 mm
+    arrival (sim/fw_checks/fw_e1_corridor_validate.py:38-44)."""
+    from scipy.signal import hilbert
+    fs = 1.0 / dt
+    e = np.abs(hilbert(x))
+    k0 = int(2 * 0.100 / C_REF * fs)
+    a, b = max(k0 - int(2e-6 * fs), 0), k0 + int(2e-6 * fs)
+    k = a + int(np.argmax(e[a:b]))
+    return float(e[k]), k * dt
+
+
+def corridor_licensed(full, corridor, dt):
+    """The reference's licence for the E1 corridor crop: corridor E1 within
+    1 % of the full disk's and its time within 20 ns
+    (sim/fw_checks/fw_e1_corridor_validate.py:114-124)."""
+    (ef, tf), (ec, tc) = e1_of(full, dt), e1_of(corridor, dt)
+    return abs(ec / ef - 1) < 0.01 and abs(tc - tf) < 20e-9
+
+
+def test_stored_corridor_trace_is_licensed_against_the_stored_full_disk():
+    """CPU: the reference's two stored 5 MHz traces satisfy its own corridor
+    licence (the crop keeps E1 within 1 % and 20 ns)."""
+    g = np.load(GOLD)
+    assert g["f5c_trace"].shape == g["f5_trace"].shape and float(g["f5c_half_w"]) == 0.027
+    assert corridor_licensed(g["f5_trace"], g["f5c_trace"], float(g["f5_dt"]))
+
+
 def _hf_case(key):
     from pefdtd import damping, specimen
     import hashlib
@@ -221,7 +251,7 @@ def _hf_case(key):
     tr = np.asarray(fdtd.forward_fused_labels(lab, run["axes"], h, dt, nt, run["src"], run["wav"], run["rec"],
                                               order=8, coeffs=c["co"], sponge_width=c["sponge"], damp_mask=c["dm"]),
                     float).ravel()
-    return c, run, tr, stored
+    return c, run, tr, stored, nd
 
 
 def test_high_frequency_traces_are_stored():
@@ -239,7 +269,7 @@ def test_3mhz_trace():
     reference's current kernels; against the stored trace correlation >
     0.999, coda level within 0.2 dB (measured 0.08), at the reference
     kernels' own distance from it."""
-    c, run, tr, stored = _hf_case("f3")
+    c, run, tr, stored, _ = _hf_case("f3")
     ref = _reference_kernels(c, 0, run)
     assert _rel(tr, ref) <= 1e-5, _rel(tr, ref)
     assert float(np.corrcoef(tr, stored)[0, 1]) > 0.999
@@ -249,11 +279,26 @@ def test_3mhz_trace():
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not os.environ.get("PE_LONG_TESTS"),
-                    reason="5 MHz: 194 M cells x 9895 steps, about two minutes of GPU time")
-def test_5mhz_trace():
+                    reason="5 MHz: 194 M + 101 M cells x 9895 steps, about four minutes of GPU time")
+def test_5mhz_trace_and_its_e1_corridor():
     """5 MHz (299 x 806 x 806 cells, 9895 steps): correlation > 0.999 with
-    the stored trace, within the stored set's offset (measured 2.4 %)."""
-    c, run, tr, stored = _hf_case("f5")
+    the stored trace, within the stored set's offset (measured 2.4 %). The
+    same run cropped by crop.e1_corridor to |y| <= 27 mm (~0.55 of the
+    cells): correlation > 0.999 with the stored corridor trace, and the
+    crop licensed against the full run by the reference's criterion."""
+    from pefdtd import crop, fdtd
+    c, run, tr, stored, nd = _hf_case("f5")
     assert np.isfinite(tr).all()
     assert float(np.corrcoef(tr, stored)[0, 1]) > 0.999
     assert _rel(tr, stored) < 0.03
+    g = c["g"]
+    cut = crop.e1_corridor(c["lab"], c["pts"], c["h"], float(g["f5c_half_w"]), damp_mask=c["dm"])
+    w = 1.0 / len(cut["pts"])
+    tc = np.asarray(fdtd.forward_fused_labels(cut["lab"], run["axes"], c["h"], run["dt"], run["nt"],
+                                              [(p, w) for p in cut["pts"]], run["wav"],
+                                              [(cut["pts"], np.full(len(cut["pts"]), w))], order=8, coeffs=c["co"],
+                                              sponge_width=c["sponge"], damp_mask=cut["damp_mask"]), float).ravel()
+    stored_c = g["f5c_trace"]
+    assert float(np.corrcoef(tc, stored_c)[0, 1]) > 0.999
+    assert _rel(tc, stored_c) < 0.03
+    assert corridor_licensed(tr, tc, run["dt"])
