@@ -345,7 +345,10 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
         solver = lambda setups, progress: solve_batch(setups, progress, device=device)  # noqa: E731
     d = sweep_dir(cfg["name"], root)
     stop_flag = os.path.join(d, "STOP")
-    if os.path.exists(stop_flag):
+    # shared files change on rank 0 alone (a stale STOP flag, config.json);
+    # the other ranks reach their first read of them after the pending-list
+    # broadcast below, which rank 0 joins only after these writes
+    if rank == 0 and os.path.exists(stop_flag):
         os.remove(stop_flag)
     if cfg.get("axes_convention") != "rigid2":
         if done_azimuths(cfg, root):
@@ -354,12 +357,13 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
                 "rigid-rotation convention would mix with the old one. Start a new sweep.")
             return "legacy"
         cfg["axes_convention"] = "rigid2"
-        p = os.path.join(d, "config.json")
-        tmp = p + ".tmp"
-        keep = {k: v for k, v in cfg.items() if not k.startswith("_")}
-        with open(tmp, "w", encoding="utf-8") as f:
-            json.dump(keep, f, indent=1)
-        _replace(tmp, p, critical=True)
+        if rank == 0:
+            p = os.path.join(d, "config.json")
+            tmp = p + ".tmp"
+            keep = {k: v for k, v in cfg.items() if not k.startswith("_")}
+            with open(tmp, "w", encoding="utf-8") as f:
+                json.dump(keep, f, indent=1)
+            _replace(tmp, p, critical=True)
 
     f0 = cfg["f0_mhz"] * 1e6
     h = C_REF / f0 / cfg["ppw"]
@@ -383,7 +387,14 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
     co = sweep_coeffs(cfg)
     todo = pending(cfg, root)
     if world > 1:
+        # every rank shards rank 0's list: a rank that read the directory
+        # after another had written files would see a shorter one, and the
+        # shares would no longer cover the pending azimuths
+        import torch.distributed as dist
         from .shard import assign
+        box = [todo]
+        dist.broadcast_object_list(box, src=0)
+        todo = box[0]
         todo = [todo[i] for i in assign([1.0] * len(todo), world)[rank]]
     log(f"[sweep] {len(todo)} of {len(azimuths(cfg))} azimuths pending"
         + (f" on rank {rank} of {world}" if world > 1 else ""))

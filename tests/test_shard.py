@@ -61,6 +61,12 @@ def _worker(rank, world, port, out_dir, mode):
             def solver(setups, progress):
                 progress(1.0)
                 return [synthetic_echo(s["nt"], s["dt"], s["f0"]).astype(float) for s in setups]
+            if rank == 1:
+                # start late: a rank that read the pending azimuths on its
+                # own after rank 0 had written its share would shard a
+                # shorter list, and azimuths would go unsolved
+                import time
+                time.sleep(3.0)
             res = sweep.run(cfg, labeller="exact", batch=2, log=lambda *a: None, solver=solver,
                             prefetch=False, rank=rank, world=world)
             dist.barrier()
@@ -95,8 +101,9 @@ def test_run_sharded_gloo_two_ranks(tmp_path):
 
 
 def test_sharded_sweep_gloo_two_ranks(tmp_path):
-    """Two ranks split the pending azimuths of one sweep; together they write
-    every az file once, and the sweep is complete for both."""
+    """Two ranks split the pending azimuths of one sweep, rank 1 starting
+    late; together they write every az file once, and the sweep is complete
+    for both."""
     from pefdtd import sweep
     res = _spawn(tmp_path, "sweep")
     assert [r["result"] for r in res] == ["complete", "complete"]
