@@ -9,10 +9,10 @@
 // (lv, ls) = dJ/d(v^n, s^n), and accumulate dJ/dC per material:
 //   k_adj_inject    lv or ls += trace adjoint at the receiver cells
 //   k_adj_vel_u     u = d dt_h lv / rho_face              (per component)
-//   k_adj_vel       ls += G^T u                           (gathers)
-//   k_adj_strain    g = D v^{n-1}                         (same taps as forward)
-//   k_adj_w         w[p][J] = sum over stresses I at position p of
+//   k_adj_vel       ls += G^T u                           (gathers), then
+//                   w[p][J] = sum over stresses I at position p of
 //                   C_IJ dt ls_I, for the 18 moved (p, J), once per cell
+//   k_adj_strain    g = D v^{n-1}                         (same taps as forward)
 //   k_adj_stress    dJ/dC[m] += dt ls (x) (M g); t = M^T C^T (dt ls);
 //                   then ls = d ls
 //   k_adj_velfin    lv = d lv + D^T t
@@ -229,6 +229,38 @@ __global__ void k_adj_vel_u(AdjArgs<T> A)
     A.u[2][i] = adj_div(s * A.lv[2][i], rvz, r0, A.rinv, m0);
 }
 
+// index of the moved (position p, strain J) pairs, p != position of J:
+// J = 0..5 in order, p ascending, three per strain
+__host__ __device__ constexpr int adj_widx(int J, int p)
+{
+    return 3 * J + (p - (p > (J < 3 ? 0 : J - 2) ? 1 : 0));
+}
+
+// w[p][J](x) = sum over I at position p of C_IJ(x) * (dt * ls_I(x)), I
+// ascending, for the moved pairs: the values the stress transpose gathers
+// from the forward cells of each move tap. ls: the cell's ls after the
+// velocity transpose, as k_adj_vel has just stored it.
+template <typename T>
+__device__ __forceinline__ void adj_w_cell(const AdjArgs<T> &A, long long i, const T (&ls)[6])
+{
+    const int VP[6] = {0, 0, 0, 1, 2, 3};
+    const T *Cx = A.c21 + (long long)(A.lab[i] & LAB_MAT) * C21_STRIDE;
+    T e[6];
+#pragma unroll
+    for (int I = 0; I < 6; ++I) e[I] = A.dt * ls[I];
+#pragma unroll
+    for (int J = 0; J < 6; ++J)
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p == VP[J]) continue;
+            T W = 0;
+#pragma unroll
+            for (int I = 0; I < 6; ++I)
+                if (VP[I] == p) W += Cx[c21_slot(I, J)] * e[I];
+            A.w[adj_widx(J, p)][i] = W;
+        }
+}
+
 template <typename T, bool GX, bool GYZ>
 __device__ __forceinline__ void adj_vel_cell(const AdjArgs<T> &A, long long i, int iz, int iy, int ix)
 {
@@ -237,12 +269,16 @@ __device__ __forceinline__ void adj_vel_cell(const AdjArgs<T> &A, long long i, i
     auto X = [&](const T *p) { return [p](int o) { return p[o]; }; };
     auto Y = [&](const T *p) { return [p, sy](int o) { return p[o * sy]; }; };
     auto Z = [&](const T *p) { return [p, sz](int o) { return p[o * sz]; }; };
-    A.ls[0][i] += DfT<T, GX>(X(ux), ix, A.nx, A.c, A.nc);
-    A.ls[1][i] += DfT<T, GYZ>(Y(uy), iy, A.ny, A.c, A.nc);
-    A.ls[2][i] += DfT<T, GYZ>(Z(uz), iz, A.nz, A.c, A.nc);
-    A.ls[3][i] += DbT<T, GYZ>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T, GYZ>(Y(uz), iy, A.ny, A.c, A.nc);
-    A.ls[4][i] += DbT<T, GYZ>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T, GX>(X(uz), ix, A.nx, A.c, A.nc);
-    A.ls[5][i] += DbT<T, GYZ>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T, GX>(X(uy), ix, A.nx, A.c, A.nc);
+    T ls[6];
+    ls[0] = A.ls[0][i] + DfT<T, GX>(X(ux), ix, A.nx, A.c, A.nc);
+    ls[1] = A.ls[1][i] + DfT<T, GYZ>(Y(uy), iy, A.ny, A.c, A.nc);
+    ls[2] = A.ls[2][i] + DfT<T, GYZ>(Z(uz), iz, A.nz, A.c, A.nc);
+    ls[3] = A.ls[3][i] + (DbT<T, GYZ>(Z(uy), iz, A.nz, A.c, A.nc) + DbT<T, GYZ>(Y(uz), iy, A.ny, A.c, A.nc));
+    ls[4] = A.ls[4][i] + (DbT<T, GYZ>(Z(ux), iz, A.nz, A.c, A.nc) + DbT<T, GX>(X(uz), ix, A.nx, A.c, A.nc));
+    ls[5] = A.ls[5][i] + (DbT<T, GYZ>(Y(ux), iy, A.ny, A.c, A.nc) + DbT<T, GX>(X(uy), ix, A.nx, A.c, A.nc));
+#pragma unroll
+    for (int I = 0; I < 6; ++I) A.ls[I][i] = ls[I];
+    adj_w_cell(A, i, ls);   // this cell's ls is final for the step until k_adj_stress damps it
 }
 template <typename T>
 __global__ void k_adj_vel(AdjArgs<T> A)
@@ -312,40 +348,6 @@ __device__ __forceinline__ bool move_ok(int z, int y, int x, int dz, int dy, int
 }
 
 // ---------------------------------------------------------------- stress transpose
-// index of the moved (position p, strain J) pairs, p != position of J:
-// J = 0..5 in order, p ascending, three per strain
-__host__ __device__ constexpr int adj_widx(int J, int p)
-{
-    return 3 * J + (p - (p > (J < 3 ? 0 : J - 2) ? 1 : 0));
-}
-
-// w[p][J](x) = sum over I at position p of C_IJ(x) * (dt * ls_I(x)), I
-// ascending, for the moved pairs: the values the stress transpose gathers
-// from the forward cells of each move tap
-template <typename T>
-__global__ void k_adj_w(AdjArgs<T> A)
-{
-    long long i;
-    int iz, iy, ix;
-    if (!adj_cell(A, i, iz, iy, ix)) return;
-    const int VP[6] = {0, 0, 0, 1, 2, 3};
-    const T *Cx = A.c21 + (long long)(A.lab[i] & LAB_MAT) * C21_STRIDE;
-    T e[6];
-#pragma unroll
-    for (int I = 0; I < 6; ++I) e[I] = A.dt * A.ls[I][i];
-#pragma unroll
-    for (int J = 0; J < 6; ++J)
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            if (p == VP[J]) continue;
-            T W = 0;
-#pragma unroll
-            for (int I = 0; I < 6; ++I)
-                if (VP[I] == p) W += Cx[c21_slot(I, J)] * e[I];
-            A.w[adj_widx(J, p)][i] = W;
-        }
-}
-
 constexpr int ADJ_STRESS_WARPS = ADJ_BY;   // k_adj_stress blocks: one warp per row of the 32 x 8 tile
 static_assert(ADJ_BX == 32, "a warp is one row of an adjoint block");
 
@@ -536,7 +538,7 @@ __global__ void __launch_bounds__(ADJ_STRESS_WARPS * 32) k_adj_stress(AdjArgs<T>
     const T *Cm = A.c21 + (long long)m * C21_STRIDE;
     if (inside) adj_strain_adjoint<T, false>(A, i, iz, iy, ix, Cm, e);
     else adj_strain_adjoint<T, true>(A, i, iz, iy, ix, Cm, e);
-    // the step's last use of ls at this cell (k_adj_w ran before, and only
+    // the step's last use of ls at this cell (k_adj_vel formed w from it, and only
     // this thread reads it here): apply the deferred damping, ls = d ls (the
     // transpose of the forward s^{n-1} * d)
     const T d = (T)adj_damp(A, iz, iy, ix, i);

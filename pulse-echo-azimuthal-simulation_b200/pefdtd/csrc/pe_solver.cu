@@ -911,7 +911,6 @@ int adjoint_step_t(PeSolver *S, const PeAdjoint *adj, int64_t n, const void *res
     pe::k_adj_vel_u<T><<<ag, ab, 0, st>>>(A);
     pe::k_adj_vel<T><<<ag, ab, 0, st>>>(A);
     pe::k_adj_strain<T><<<ag, ab, 0, st>>>(A);
-    pe::k_adj_w<T><<<ag, ab, 0, st>>>(A);
     pe::k_adj_stress<T><<<ag, ab, 0, st>>>(A);
     pe::k_adj_velfin<T><<<ag, ab, 0, st>>>(A);
     PE_CUDA(cudaGetLastError());
