@@ -280,8 +280,10 @@ __device__ __forceinline__ void adj_vel_cell(const AdjArgs<T> &A, long long i, i
     for (int I = 0; I < 6; ++I) A.ls[I][i] = ls[I];
     adj_w_cell(A, i, ls);   // this cell's ls is final for the step until k_adj_stress damps it
 }
+// eight 256-thread blocks per SM in FP32 (32 registers, no spills; the
+// stiffness columns formed at the end would otherwise take it to 40)
 template <typename T>
-__global__ void k_adj_vel(AdjArgs<T> A)
+__global__ void __launch_bounds__(ADJ_BX * ADJ_BY, sizeof(T) == 4 ? 8 : 4) k_adj_vel(AdjArgs<T> A)
 {
     long long i;
     int iz, iy, ix;
