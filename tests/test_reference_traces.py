@@ -176,14 +176,16 @@ def test_every_fabric_matches_the_reference_kernels(ladder_case, k):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rot", [17, 76])
+@pytest.mark.parametrize("rot", [17, 31, 47, 76])
 def test_azimuth_traces_with_the_rotation_they_were_made_with(ladder_case, rot):
     """The specimen rotated by rot degrees (`rotated_grid`: the grid's
     digest, and its c-axes those of the reference's current code): with the
     c-axes rotated as the stored traces were (axes @ R.T), within 1e-5 of the
     reference's current kernels on the same inputs and correlated > 0.999
     with the stored trace (76 degrees is the reference's beam walk-off
-    outlier: coda level -22 dB against -45 and -53 dB at 62 and 90)."""
+    outlier: coda level -22 dB against -45 and -53 dB at 62 and 90). At 62
+    degrees the solve is as close to the reference's kernels but correlates
+    0.9990 with the stored trace, just under this bound; 90 is not run."""
     import hashlib
     from pefdtd import damping, specimen
     c = ladder_case
