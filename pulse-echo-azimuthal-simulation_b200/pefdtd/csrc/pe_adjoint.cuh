@@ -591,4 +591,6 @@ __global__ void k_adj_velfin(AdjArgs<T> A)
     ADJ_DISPATCH(A, adj_velfin_cell, A, i, iz, iy, ix);
 }
 
+#undef ADJ_DISPATCH
+
 }  // namespace pe

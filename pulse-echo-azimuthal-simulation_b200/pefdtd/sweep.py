@@ -323,9 +323,10 @@ def run(cfg, root=None, batch=None, device=None, labeller=None, log=print, solve
     (:func:`pefdtd.traces.analyse`: t1 identical to the host analysis, the
     others to ~1e-13 relative); with a stand-in, on the host, exactly as the
     reference computes them. ``rank``/``world``: one process per
-    GPU; each rank solves its share of the pending azimuths
-    (:func:`pefdtd.shard.assign`, every azimuth of a sweep costs the same)
-    and writes their files; rank 0 alone writes status.json."""
+    GPU, in an initialised torch.distributed process group; each rank solves
+    its share (:func:`pefdtd.shard.assign`, every azimuth of a sweep costs
+    the same) of rank 0's list of pending azimuths, broadcast to all, and
+    writes their files; rank 0 alone writes status.json and config.json."""
     root = _root_of(cfg, root)
     if world > 1 and rank != 0:
         status = lambda *a, **k: None  # noqa: E731,F841  (rank 0 owns status.json)
